@@ -1,0 +1,397 @@
+"""Benchmark of the lattice-Boltzmann hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload cylinder_channel|kelvin_helmholtz|taylor_green_3d]
+                    [--storage f32|f16|bf16|f64]
+
+One bench step is one AA step pair (two LBM time steps: the even and the odd kernel), the
+smallest unit after which the populations are back in the reference's standard layout.
+The metric is MLUPS = cells x LBM steps / s, counting every cell (walls included) as the
+reference's run_sim does (python/boltzmann/simulation.py:245-246).
+
+Default workload: D2Q9 TRT cylinder channel 4096x2048 with a Boussinesq-coupled D2Q5 tracer,
+FP32 -- seeded synthetic inputs of that configuration. Its populations (302 MB + 168 MB) exceed
+the 126 MB L2, so no flush is needed between steps.
+
+``--impl reference`` times the reference's own kernels (src/lib.cl compiled as C++, the CPU
+checker in oracle/_ref) on all host cores for the same workload, on a bounded number of steps.
+Multi-GPU (torchrun): every rank runs an independent replica (the path has no exchange step);
+value is the aggregate over ranks, timed as the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def measured_peaks() -> tuple[dict, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+def make_setup(workload: str):
+    from boltzmann_b200 import workloads
+
+    if workload == "cylinder_channel":
+        return workloads.cylinder_channel()
+    if workload == "kelvin_helmholtz":
+        return workloads.kelvin_helmholtz()
+    if workload == "taylor_green_3d":
+        return workloads.taylor_green_3d()
+    raise SystemExit(f"unknown workload {workload}")
+
+
+def algorithmic_bytes_per_cell(setup, storage: str) -> float:
+    """Population bytes read + written per cell update (+ the coupled tracer value, read and
+    written every step). Flags and the end-of-call rho/vel writes are not counted."""
+    q = 9 if len(setup.counts) == 2 else 27
+    qt = 5 if len(setup.counts) == 2 else 7
+    pop = {"f32": 4, "f16": 2, "bf16": 2, "f64": 8}[storage]
+    real = 8 if storage == "f64" else 4
+    b = 2 * q * pop + len(setup.tracers) * 2 * qt * real
+    if setup.couplings:
+        b += 2 * real
+    return float(b)
+
+
+def profiled_traffic(kernel_tag: str) -> float | None:
+    """DRAM bytes per cell update from the committed ncu summary of this kernel, if any."""
+    for p in sorted((ROOT / "profiles").glob(f"*{kernel_tag}*.md")):
+        m = re.search(r"dram_bytes_per_cell_update:\s*([0-9.]+)", p.read_text())
+        if m:
+            return float(m.group(1))
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, device: int) -> None:
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"),
+                stderr=subprocess.DEVNULL,
+            )
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self) -> dict:
+        if self.path is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {
+            "sm_mhz": statistics.median(sm),
+            "sm_max_mhz": max(smax),
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def omega_for(kind: str, tau: float):
+    from boltzmann_b200.core import bgk, trt
+
+    return bgk(tau) if kind == "bgk" else trt(tau)
+
+
+def build_sim(setup, storage: str):
+    from boltzmann_b200 import workloads
+    from boltzmann_b200.core import Simulation
+
+    sim = Simulation("gpu", setup.counts, omega_for(setup.collision, setup.tau), storage=storage)
+    workloads.apply(sim, setup, omega_for)
+    return sim
+
+
+def cpu_reference_rate(setup, budget_s: float, max_pairs: int | None = None) -> dict:
+    """MLUPS of the reference kernels compiled as C++ (oracle/_ref), all host threads."""
+    from boltzmann_b200 import workloads
+    from oracle import build as oracle_build
+    from oracle.oracle import Omega, OracleSimulation, default_threads, reference_available
+
+    oracle_build.build_ref()
+    kind = "reference" if reference_available() else "port"
+    threads = default_threads()
+
+    def om(k, tau):
+        return Omega.bgk(tau) if k == "bgk" else Omega.trt(tau)
+
+    sim = OracleSimulation(setup.counts, om(setup.collision, setup.tau), backend=kind,
+                           nthreads=threads)
+
+    def tracer_handle(s, name, o):
+        return name, s.add_tracer(name, o).val
+
+    workloads.apply(sim, setup, om, tracer_handle)
+    t0 = time.perf_counter()
+    sim.iterate(2)  # first pair: equilibrate + one AA pair (untimed warm-up)
+    first = time.perf_counter() - t0
+    pairs = max(1, int(budget_s / max(first, 1e-3)))
+    if max_pairs is not None:
+        pairs = min(pairs, max_pairs)
+    t0 = time.perf_counter()
+    sim.iterate(2 * pairs)
+    dt = time.perf_counter() - t0
+    mlups = setup.cells * 2 * pairs / dt / 1e6
+    return {
+        "value": mlups,
+        "unit": "MLUPS",
+        "cores": threads,
+        "kind": kind,
+        "sample": f"{setup.name} {'x'.join(map(str, setup.counts))}, {2 * pairs} LBM steps "
+        f"(full domain) after one untimed step pair; {threads} OpenMP threads",
+        "pairs": pairs,
+        "seconds": dt,
+    }
+
+
+def dist_env() -> tuple[int, int, int]:
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def run_reference(args) -> None:
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    setup = make_setup(args.workload)
+    # Bounded: the whole arm stays within a few minutes.
+    base = cpu_reference_rate(setup, budget_s=min(60.0, 2.0 * max(args.steps, 1)),
+                              max_pairs=args.steps)
+    line = {
+        "impl": "reference",
+        "metric": "MLUPS",
+        "value": base["value"],
+        "unit": "MLUPS",
+        "n_gpus": args.gpus,
+        "steps": base["pairs"],
+        "warmup": 1,
+        "ms_per_step": 1e3 * base["seconds"] / base["pairs"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": config_block(setup, "f32", world),
+        "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": base["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_block(setup, storage: str, world: int) -> dict:
+    return {
+        "workload": f"{setup.name} {'x'.join(map(str, setup.counts))}"
+        + (" + D2Q5 tracer + Boussinesq" if setup.tracers else ""),
+        "lattice": "D2Q9" if len(setup.counts) == 2 else "D3Q27",
+        "collision": setup.collision,
+        "storage": storage,
+        "cells": setup.cells,
+        "lbm_steps_per_bench_step": 2,
+        "l2": "inputs larger than L2 (populations > 126 MB); no flush",
+        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+    }
+
+
+def run_ours(args) -> None:
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    setup = make_setup(args.workload)
+    K, W = args.steps, max(args.warmup, 3)
+
+    # Device-timed run: inputs resident in HBM, only the AA kernels in the timed region.
+    sim = build_sim(setup, args.storage)
+    sim.iterate(2 * W)  # upload, equilibrate, warm-up steps
+    stream = torch.cuda.ExternalStream(sim._stream())
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    sim._synchronize()
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        sim._iterate_device(2 * K)
+        stop.record(stream)
+        stop.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    elapsed_ms = max_over_ranks(start.elapsed_time(stop))
+    sim.iterate(2)  # read back; checks the state is still finite
+    finite = bool(np.isfinite(sim.fluid.rho).all())
+    del sim
+
+    lbm_steps = 2 * K
+    value = world * setup.cells * lbm_steps / (elapsed_ms * 1e-3) / 1e6
+    launch_ms = elapsed_ms / lbm_steps
+    bpc = algorithmic_bytes_per_cell(setup, args.storage)
+    peaks, peak_kind = measured_peaks()
+    achieved = bpc * setup.cells / (launch_ms * 1e-3) / 1e9
+    tag = {"cylinder_channel": "d2q9_trt_tracer", "kelvin_helmholtz": "d2q9_bgk",
+           "taylor_green_3d": "d3q27_bgk"}[args.workload] + f"_{args.storage}"
+    traffic_pc = profiled_traffic(tag)
+
+    # End to end through the public API with host buffers: a fresh Simulation from host arrays;
+    # one iterate(2K) call uploads flags/rho/vel/C, equilibrates, steps and reads rho/vel/C back.
+    sim2 = build_sim(setup, args.storage)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim2.iterate(lbm_steps)
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    n = setup.cells
+    d = len(setup.counts)
+    nt = len(setup.tracers)
+    h2d = n * (1 + d) * 4 + n * 4 + nt * n * 4  # flags (sent as i32), rho, vel, tracer C
+    d2h = n * (1 + d) * 4 + nt * n * 4
+    e2e_value = world * n * lbm_steps / e2e_s / 1e6
+    del sim2
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_rate(setup, budget_s=args.cpu_seconds)
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        line = {
+            "metric": "MLUPS",
+            "value": value,
+            "unit": "MLUPS",
+            "n_gpus": world,
+            "steps": K,
+            "warmup": W,
+            "ms_per_step": elapsed_ms / K,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": {"f32": "f32", "f16": "f16-offset storage, f32 compute",
+                      "bf16": "bf16-offset storage, f32 compute", "f64": "f64"}[args.storage],
+            "data": "synthetic",
+            "config": config_block(setup, args.storage, world),
+            "roofline": {
+                "bound": "hbm",
+                "achieved": achieved,
+                "peak": peaks["hbm_gbs"],
+                "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"],
+                "traffic": None if traffic_pc is None else traffic_pc * setup.cells,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "algorithmic_bytes_per_cell_update": bpc,
+                "kernel": f"aa_step_kernel ({tag})",
+                "frac_of_nominal_8tbs": achieved / 8000.0,
+            },
+            "cpu_baseline": cpu,
+            "e2e": {
+                "value": e2e_value,
+                "unit": "MLUPS",
+                "h2d_bytes_per_step": h2d / K,
+                "d2h_bytes_per_step": d2h / K,
+                "how": f"fresh Simulation from host arrays, one iterate({lbm_steps}) call "
+                "(upload + equilibrate + steps + read-back), host wall clock",
+            },
+            "gpu_launches": lbm_steps,
+            "clocks": clocks.summary(),
+            "finite": finite,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cylinder_channel",
+                    choices=["cylinder_channel", "kelvin_helmholtz", "taylor_green_3d"])
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f64"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

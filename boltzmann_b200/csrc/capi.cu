@@ -1,0 +1,438 @@
+// C ABI of include/lbm_cuda.h: simulation lifetime, transfers and the per-step launch loop.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/lbm_cuda.h"
+#include "aa_step.cuh"
+#include "sim.h"
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string& msg) {
+  g_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+  return fail(LBM_ERR_CUDA, std::string("CUDA error in ") + where + ": " + cudaGetErrorName(e) +
+                                " (" + cudaGetErrorString(e) + ")");
+}
+
+#define LBM_CUDA(call)                                \
+  do {                                                \
+    cudaError_t e_ = (call);                          \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+// Velocity sets known to the reference (src/velocities.rs:55-64).
+bool known_set(int d, int q) {
+  return (d == 1 && q == 3) || (d == 2 && (q == 9 || q == 5)) || (d == 3 && (q == 7 || q == 27));
+}
+
+// Sets that have a fluid update kernel (src/opencl.rs:123-129, plus D3Q27 TRT).
+bool fluid_kernel(int d, int q) { return (d == 2 && q == 9) || (d == 3 && q == 27); }
+
+// Sets that have a tracer update kernel: BGK D2Q5 / D3Q7 (src/opencl.rs:123-129).
+bool tracer_kernel(int d, int q, int collision) {
+  return collision == LBM_BGK && ((d == 2 && q == 5) || (d == 3 && q == 7));
+}
+
+int activate(lbm_sim* s) {
+  if (s == nullptr) return fail(LBM_ERR_ARGUMENT, "null simulation handle");
+  cudaError_t e = cudaSetDevice(s->device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  return LBM_OK;
+}
+
+int check_tracer(lbm_sim* s, int t) {
+  if (t < 0 || t >= (int)s->tracers.size()) return fail(LBM_ERR_ARGUMENT, "no such tracer index");
+  return LBM_OK;
+}
+
+// Host float -> device real (float, or double through a temporary for F64).
+int upload_reals(lbm_sim* s, void* dst, const float* src, int64_t count) {
+  if (s->storage != LBM_STORAGE_F64) {
+    LBM_CUDA(cudaMemcpyAsync(dst, src, count * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+    return LBM_OK;
+  }
+  float* tmp = nullptr;
+  LBM_CUDA(cudaMallocAsync((void**)&tmp, count * sizeof(float), s->stream));
+  LBM_CUDA(cudaMemcpyAsync(tmp, src, count * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+  LBM_CUDA(lbm::widen_to_double(tmp, static_cast<double*>(dst), count, s->stream));
+  LBM_CUDA(cudaFreeAsync(tmp, s->stream));
+  return LBM_OK;
+}
+
+// Device real -> host float.
+int download_reals(lbm_sim* s, float* dst, const void* src, int64_t count) {
+  if (s->storage != LBM_STORAGE_F64) {
+    LBM_CUDA(cudaMemcpyAsync(dst, src, count * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    return LBM_OK;
+  }
+  float* tmp = nullptr;
+  LBM_CUDA(cudaMallocAsync((void**)&tmp, count * sizeof(float), s->stream));
+  LBM_CUDA(lbm::narrow_to_float(static_cast<const double*>(src), tmp, count, s->stream));
+  LBM_CUDA(cudaMemcpyAsync(dst, tmp, count * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+  LBM_CUDA(cudaFreeAsync(tmp, s->stream));
+  return LBM_OK;
+}
+
+void release(lbm_sim* s) {
+  for (lbm_sim::Tracer& t : s->tracers) {
+    cudaFree(t.g);
+    cudaFree(t.val);
+  }
+  cudaFree(s->f);
+  cudaFree(s->rho);
+  cudaFree(s->vel);
+  cudaFree(s->flags);
+  cudaFree(s->status);
+  if (s->stream) cudaStreamDestroy(s->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* lbm_last_error(void) { return g_error.c_str(); }
+
+int lbm_abi_version(void) { return 1; }
+
+int lbm_create(int dim, const int64_t* counts, int q, int collision, float omega_pos,
+               float omega_neg, int storage, lbm_sim** out) {
+  if (out == nullptr || counts == nullptr) return fail(LBM_ERR_ARGUMENT, "null argument");
+  *out = nullptr;
+  if (dim < 1 || dim > 3)
+    return fail(LBM_ERR_ARGUMENT, "Invalid number of dimensions. Expected either 1, 2 or 3.");
+  if (!known_set(dim, q))
+    return fail(LBM_ERR_ARGUMENT,
+                "Unknown model: D" + std::to_string(dim) + "Q" + std::to_string(q));
+  if (collision != LBM_BGK && collision != LBM_TRT)
+    return fail(LBM_ERR_ARGUMENT, "unknown collision operator");
+  if (storage < LBM_STORAGE_F32 || storage > LBM_STORAGE_F64)
+    return fail(LBM_ERR_ARGUMENT, "unknown storage kind");
+  int64_t n = 1;
+  for (int k = 0; k < dim; ++k) {
+    if (counts[k] <= 0 || counts[k] > (1 << 30))
+      return fail(LBM_ERR_ARGUMENT, "cell counts must be positive");
+    n *= counts[k];
+  }
+  if (n > (int64_t)1 << 40) return fail(LBM_ERR_ARGUMENT, "domain too large");
+
+  lbm_sim* s = new (std::nothrow) lbm_sim();
+  if (s == nullptr) return fail(LBM_ERR_ARGUMENT, "out of host memory");
+  s->dim = dim;
+  s->q = q;
+  s->collision = collision;
+  s->storage = storage;
+  for (int k = 0; k < dim; ++k) s->counts[k] = counts[k];
+  s->n = n;
+  s->om_pos = omega_pos;
+  s->om_neg = omega_neg;
+
+  auto bail = [&](cudaError_t e, const char* where) {
+    release(s);
+    delete s;
+    return cuda_fail(e, where);
+  };
+  cudaError_t e = cudaGetDevice(&s->device);
+  if (e != cudaSuccess) return bail(e, "cudaGetDevice");
+  e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return bail(e, "cudaStreamCreate");
+  const size_t rb = s->real_bytes();
+  if ((e = cudaMalloc(&s->f, (size_t)n * q * lbm::pop_bytes(storage))) != cudaSuccess)
+    return bail(e, "cudaMalloc(f)");
+  if ((e = cudaMalloc(&s->rho, (size_t)n * rb)) != cudaSuccess) return bail(e, "cudaMalloc(rho)");
+  if ((e = cudaMalloc(&s->vel, (size_t)n * dim * rb)) != cudaSuccess)
+    return bail(e, "cudaMalloc(vel)");
+  if ((e = cudaMalloc((void**)&s->flags, (size_t)n)) != cudaSuccess)
+    return bail(e, "cudaMalloc(flags)");
+  if ((e = cudaMalloc((void**)&s->status, 64 * sizeof(double))) != cudaSuccess)
+    return bail(e, "cudaMalloc(status)");
+  s->sums = reinterpret_cast<double*>(s->status) + 1;  // 63 doubles after the status word
+  s->sums_len = 63;
+  // Reference defaults (src/fields.rs:75-77, src/simulation.rs:35): f = 0, rho = 1, vel = 0,
+  // flags = 0.
+  if ((e = cudaMemsetAsync(s->f, 0, (size_t)n * q * lbm::pop_bytes(storage), s->stream)) ||
+      (e = lbm::fill_value(s->rho, n, 1.0, storage == LBM_STORAGE_F64, s->stream)) ||
+      (e = cudaMemsetAsync(s->vel, 0, (size_t)n * dim * rb, s->stream)) ||
+      (e = cudaMemsetAsync(s->flags, 0, (size_t)n, s->stream)) ||
+      (e = cudaMemsetAsync(s->status, 0, 64 * sizeof(double), s->stream)) ||
+      (e = cudaStreamSynchronize(s->stream)))
+    return bail(e, "initialise fields");
+  *out = s;
+  return LBM_OK;
+}
+
+int lbm_destroy(lbm_sim* sim) {
+  if (sim == nullptr) return LBM_OK;
+  cudaSetDevice(sim->device);
+  cudaStreamSynchronize(sim->stream);
+  release(sim);
+  delete sim;
+  return LBM_OK;
+}
+
+int lbm_device_info(lbm_sim* sim, char* buf, int len) {
+  if (int rc = activate(sim)) return rc;
+  cudaDeviceProp p;
+  LBM_CUDA(cudaGetDeviceProperties(&p, sim->device));
+  if (buf && len > 0) std::snprintf(buf, (size_t)len, "NVIDIA %s GPU", p.name);
+  return LBM_OK;
+}
+
+int lbm_device_bytes(lbm_sim* sim, int64_t* out) {
+  if (int rc = activate(sim)) return rc;
+  const int64_t n = sim->n, rb = (int64_t)sim->real_bytes();
+  int64_t b = n * sim->q * (int64_t)lbm::pop_bytes(sim->storage) + n * rb * (1 + sim->dim) + n;
+  for (const lbm_sim::Tracer& t : sim->tracers) b += n * rb * (t.q + 1);
+  *out = b;
+  return LBM_OK;
+}
+
+int lbm_add_tracer(lbm_sim* sim, int q, int collision, float omega_pos, float omega_neg,
+                   int* out_index) {
+  if (int rc = activate(sim)) return rc;
+  (void)omega_neg;
+  if (!known_set(sim->dim, q))
+    return fail(LBM_ERR_ARGUMENT,
+                "Unknown model: D" + std::to_string(sim->dim) + "Q" + std::to_string(q));
+  if ((int)sim->tracers.size() >= lbm::kMaxTracers)
+    return fail(LBM_ERR_UNSUPPORTED, "at most " + std::to_string(lbm::kMaxTracers) +
+                                         " tracers per simulation");
+  lbm_sim::Tracer t;
+  t.q = q;
+  t.collision = collision;
+  t.omega = omega_pos;
+  const size_t rb = sim->real_bytes();
+  LBM_CUDA(cudaMalloc(&t.g, (size_t)sim->n * q * rb));
+  cudaError_t e = cudaMalloc(&t.val, (size_t)sim->n * rb);
+  if (e != cudaSuccess) {
+    cudaFree(t.g);
+    return cuda_fail(e, "cudaMalloc(tracer val)");
+  }
+  LBM_CUDA(cudaMemsetAsync(t.g, 0, (size_t)sim->n * q * rb, sim->stream));
+  LBM_CUDA(cudaMemsetAsync(t.val, 0, (size_t)sim->n * rb, sim->stream));
+  sim->tracers.push_back(t);
+  if (out_index) *out_index = (int)sim->tracers.size() - 1;
+  return LBM_OK;
+}
+
+int lbm_set_gravity(lbm_sim* sim, const float* g) {
+  if (int rc = activate(sim)) return rc;
+  if (g == nullptr) return fail(LBM_ERR_ARGUMENT, "null gravity");
+  sim->has_gravity = true;
+  for (int k = 0; k < sim->dim; ++k) sim->gravity[k] = g[k];
+  return LBM_OK;
+}
+
+int lbm_add_coupling(lbm_sim* sim, int tracer, float alpha, float c0, const float* g) {
+  if (int rc = activate(sim)) return rc;
+  if (int rc = check_tracer(sim, tracer)) return rc;
+  if (g == nullptr) return fail(LBM_ERR_ARGUMENT, "null gravity");
+  lbm_sim::Coupling c;
+  c.tracer = tracer;
+  c.alpha = alpha;
+  c.c0 = c0;
+  for (int k = 0; k < sim->dim; ++k) c.g[k] = g[k];
+  sim->couplings.push_back(c);
+  return LBM_OK;
+}
+
+int lbm_upload_flags(lbm_sim* sim, const int32_t* flags) {
+  if (int rc = activate(sim)) return rc;
+  if (flags == nullptr) return fail(LBM_ERR_ARGUMENT, "null flags");
+  // Only bits 0-3 are read by the kernels (WALL, FIXED_FLUID_*, FIXED_SCALAR_VALUE).
+  std::vector<uint8_t> low((size_t)sim->n);
+  for (int64_t i = 0; i < sim->n; ++i) low[(size_t)i] = (uint8_t)(flags[i] & 0xF);
+  LBM_CUDA(cudaMemcpyAsync(sim->flags, low.data(), (size_t)sim->n, cudaMemcpyHostToDevice,
+                           sim->stream));
+  LBM_CUDA(cudaStreamSynchronize(sim->stream));
+  return LBM_OK;
+}
+
+int lbm_upload_fluid(lbm_sim* sim, const float* rho, const float* vel) {
+  if (int rc = activate(sim)) return rc;
+  if (rho) {
+    if (int rc = upload_reals(sim, sim->rho, rho, sim->n)) return rc;
+  }
+  if (vel) {
+    if (int rc = upload_reals(sim, sim->vel, vel, sim->n * sim->dim)) return rc;
+  }
+  LBM_CUDA(cudaStreamSynchronize(sim->stream));
+  return LBM_OK;
+}
+
+int lbm_upload_tracer(lbm_sim* sim, int tracer, const float* val) {
+  if (int rc = activate(sim)) return rc;
+  if (int rc = check_tracer(sim, tracer)) return rc;
+  if (int rc = upload_reals(sim, sim->tracers[tracer].val, val, sim->n)) return rc;
+  LBM_CUDA(cudaStreamSynchronize(sim->stream));
+  return LBM_OK;
+}
+
+int lbm_equilibrate(lbm_sim* sim) {
+  if (int rc = activate(sim)) return rc;
+  cudaError_t e = lbm::equilibrate(*sim);
+  if (e == cudaErrorNotSupported) return fail(LBM_ERR_UNSUPPORTED, "no equilibrium for this set");
+  if (e != cudaSuccess) return cuda_fail(e, "equilibrate");
+  return LBM_OK;
+}
+
+int lbm_equilibrate_tracer(lbm_sim* sim, int tracer) {
+  if (int rc = activate(sim)) return rc;
+  if (int rc = check_tracer(sim, tracer)) return rc;
+  cudaError_t e = lbm::equilibrate_tracer(*sim, tracer);
+  if (e == cudaErrorNotSupported) return fail(LBM_ERR_UNSUPPORTED, "no equilibrium for this set");
+  if (e != cudaSuccess) return cuda_fail(e, "equilibrate_tracer");
+  return LBM_OK;
+}
+
+static int transfer_populations(lbm_sim* sim, int tracer, float* host, bool to_device) {
+  if (int rc = activate(sim)) return rc;
+  if (tracer >= 0) {
+    if (int rc = check_tracer(sim, tracer)) return rc;
+  }
+  const int q = tracer < 0 ? sim->q : sim->tracers[tracer].q;
+  const size_t bytes = (size_t)sim->n * q * sizeof(float);
+  float* tmp = nullptr;
+  LBM_CUDA(cudaMallocAsync((void**)&tmp, bytes, sim->stream));
+  cudaError_t e;
+  if (to_device) {
+    e = cudaMemcpyAsync(tmp, host, bytes, cudaMemcpyHostToDevice, sim->stream);
+    if (e == cudaSuccess) e = lbm::populations_from_aos(*sim, tracer, tmp);
+  } else {
+    e = lbm::populations_to_aos(*sim, tracer, tmp);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, bytes, cudaMemcpyDeviceToHost, sim->stream);
+  }
+  cudaFreeAsync(tmp, sim->stream);
+  if (e == cudaErrorNotSupported) return fail(LBM_ERR_UNSUPPORTED, "no layout for this set");
+  if (e != cudaSuccess) return cuda_fail(e, "populations transfer");
+  LBM_CUDA(cudaStreamSynchronize(sim->stream));
+  return LBM_OK;
+}
+
+int lbm_upload_f(lbm_sim* sim, const float* f) {
+  return transfer_populations(sim, -1, const_cast<float*>(f), true);
+}
+int lbm_download_f(lbm_sim* sim, float* f) { return transfer_populations(sim, -1, f, false); }
+int lbm_upload_g(lbm_sim* sim, int tracer, const float* g) {
+  return transfer_populations(sim, tracer < 0 ? -2 : tracer, const_cast<float*>(g), true);
+}
+int lbm_download_g(lbm_sim* sim, int tracer, float* g) {
+  return transfer_populations(sim, tracer < 0 ? -2 : tracer, g, false);
+}
+
+int lbm_iterate(lbm_sim* sim, int64_t iters) {
+  if (int rc = activate(sim)) return rc;
+  if (iters < 0 || iters % 2 != 0) return fail(LBM_ERR_ARGUMENT, "iters must be even");
+  if (iters == 0) return LBM_OK;  // no kernel is looked up when no step runs
+  if (!fluid_kernel(sim->dim, sim->q))
+    return fail(LBM_ERR_UNSUPPORTED, "Kernel not found: D" + std::to_string(sim->dim) + "Q" +
+                                         std::to_string(sim->q) + " NavierStokes");
+  for (const lbm_sim::Tracer& t : sim->tracers)
+    if (!tracer_kernel(sim->dim, t.q, t.collision))
+      return fail(LBM_ERR_UNSUPPORTED, "Kernel not found: D" + std::to_string(sim->dim) + "Q" +
+                                           std::to_string(t.q) + " AdvectionDiffusion");
+  for (int64_t it = 0; it < iters; ++it) {
+    const bool even = (it % 2) == 0;  // src/simulation.rs:350
+    const bool last = it == iters - 1;
+    cudaError_t e = sim->dim == 2 ? lbm::launch_step_d2q9(*sim, even, last)
+                                  : lbm::launch_step_d3q27(*sim, even, last);
+    if (e != cudaSuccess) return cuda_fail(e, "AA step launch");
+  }
+  return LBM_OK;
+}
+
+int lbm_download_fluid(lbm_sim* sim, float* rho, float* vel) {
+  if (int rc = activate(sim)) return rc;
+  if (rho) {
+    if (int rc = download_reals(sim, rho, sim->rho, sim->n)) return rc;
+  }
+  if (vel) {
+    if (int rc = download_reals(sim, vel, sim->vel, sim->n * sim->dim)) return rc;
+  }
+  LBM_CUDA(cudaStreamSynchronize(sim->stream));
+  return LBM_OK;
+}
+
+int lbm_download_tracer(lbm_sim* sim, int tracer, float* val) {
+  if (int rc = activate(sim)) return rc;
+  if (int rc = check_tracer(sim, tracer)) return rc;
+  if (int rc = download_reals(sim, val, sim->tracers[tracer].val, sim->n)) return rc;
+  LBM_CUDA(cudaStreamSynchronize(sim->stream));
+  return LBM_OK;
+}
+
+int lbm_download_fluid_f64(lbm_sim* sim, double* rho, double* vel) {
+  if (int rc = activate(sim)) return rc;
+  if (sim->storage != LBM_STORAGE_F64)
+    return fail(LBM_ERR_STATE, "lbm_download_fluid_f64 needs LBM_STORAGE_F64");
+  if (rho)
+    LBM_CUDA(cudaMemcpyAsync(rho, sim->rho, sim->n * sizeof(double), cudaMemcpyDeviceToHost,
+                             sim->stream));
+  if (vel)
+    LBM_CUDA(cudaMemcpyAsync(vel, sim->vel, sim->n * sim->dim * sizeof(double),
+                             cudaMemcpyDeviceToHost, sim->stream));
+  LBM_CUDA(cudaStreamSynchronize(sim->stream));
+  return LBM_OK;
+}
+
+int lbm_conservation(lbm_sim* sim, double* out, int len) {
+  if (int rc = activate(sim)) return rc;
+  const int need = 1 + sim->dim + (int)sim->tracers.size();
+  if (out == nullptr || len < need)
+    return fail(LBM_ERR_ARGUMENT, "output needs 1 + dim + ntracers doubles");
+  LBM_CUDA(cudaMemsetAsync(sim->sums, 0, need * sizeof(double), sim->stream));
+  cudaError_t e = lbm::conservation_sums(*sim, sim->sums);
+  if (e == cudaErrorNotSupported) return fail(LBM_ERR_UNSUPPORTED, "no sums for this set");
+  if (e != cudaSuccess) return cuda_fail(e, "conservation sums");
+  LBM_CUDA(cudaMemcpyAsync(out, sim->sums, need * sizeof(double), cudaMemcpyDeviceToHost,
+                           sim->stream));
+  LBM_CUDA(cudaStreamSynchronize(sim->stream));
+  return LBM_OK;
+}
+
+int lbm_nonfinite(lbm_sim* sim, int* out) {
+  if (int rc = activate(sim)) return rc;
+  int word = 0;
+  LBM_CUDA(cudaMemcpyAsync(&word, sim->status, sizeof(int), cudaMemcpyDeviceToHost, sim->stream));
+  LBM_CUDA(cudaMemsetAsync(sim->status, 0, sizeof(int), sim->stream));
+  LBM_CUDA(cudaStreamSynchronize(sim->stream));
+  if (out) *out = word & 1;
+  return LBM_OK;
+}
+
+int lbm_synchronize(lbm_sim* sim) {
+  if (int rc = activate(sim)) return rc;
+  LBM_CUDA(cudaStreamSynchronize(sim->stream));
+  return LBM_OK;
+}
+
+int lbm_stream(lbm_sim* sim, void** stream) {
+  if (int rc = activate(sim)) return rc;
+  if (stream) *stream = (void*)sim->stream;
+  return LBM_OK;
+}
+
+void* lbm_host_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (cudaMallocHost(&p, bytes ? bytes : 1) != cudaSuccess) {
+    g_error = "cudaMallocHost failed";
+    return nullptr;
+  }
+  return p;
+}
+
+void lbm_host_free(void* ptr) {
+  if (ptr) cudaFreeHost(ptr);
+}
+
+}  // extern "C"

@@ -1,0 +1,65 @@
+// Internal state behind the lbm_sim handle of include/lbm_cuda.h.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+struct lbm_sim {
+  struct Tracer {
+    int q = 0;
+    int collision = 0;
+    float omega = 0;
+    void* g = nullptr;    // [q][N], float (double for F64 storage)
+    void* val = nullptr;  // [N]
+  };
+  struct Coupling {
+    int tracer = 0;
+    float alpha = 0, c0 = 0;
+    float g[3] = {0, 0, 0};
+  };
+
+  int dim = 0, q = 0, collision = 0, storage = 0;
+  int64_t counts[3] = {1, 1, 1};
+  int64_t n = 0;  // cell count
+  float om_pos = 0, om_neg = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+
+  void* f = nullptr;    // [q][N] populations in the storage type
+  void* rho = nullptr;  // [N], float (double for F64)
+  void* vel = nullptr;  // [N][dim]
+  uint8_t* flags = nullptr;
+  int* status = nullptr;      // device word: bit 0 = non-finite density seen
+  double* sums = nullptr;     // device scratch of the conservation reduction
+  int sums_len = 0;
+
+  std::vector<Tracer> tracers;
+  bool has_gravity = false;
+  float gravity[3] = {0, 0, 0};
+  std::vector<Coupling> couplings;
+
+  size_t real_bytes() const { return storage == 3 ? 8 : 4; }
+};
+
+namespace lbm {
+
+// Bytes of one stored population for a storage kind.
+inline size_t pop_bytes(int storage) { return storage == 3 ? 8 : (storage == 0 ? 4 : 2); }
+
+// Enqueues one AA step of the whole simulation (fluid, tracers, sources) on sim.stream.
+cudaError_t launch_step_d2q9(const lbm_sim& sim, bool even, bool write_moments);
+cudaError_t launch_step_d3q27(const lbm_sim& sim, bool even, bool write_moments);
+
+// Field kernels (fields.cu), all on sim.stream.
+cudaError_t equilibrate(const lbm_sim& sim);
+cudaError_t equilibrate_tracer(const lbm_sim& sim, int tracer);
+cudaError_t populations_from_aos(const lbm_sim& sim, int tracer, const float* d_aos);
+cudaError_t populations_to_aos(const lbm_sim& sim, int tracer, float* d_aos);
+cudaError_t narrow_to_float(const double* src, float* dst, int64_t count, cudaStream_t s);
+cudaError_t widen_to_double(const float* src, double* dst, int64_t count, cudaStream_t s);
+cudaError_t fill_value(void* dst, int64_t count, double value, bool is_double, cudaStream_t s);
+cudaError_t conservation_sums(const lbm_sim& sim, double* d_out);
+
+}  // namespace lbm

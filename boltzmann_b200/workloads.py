@@ -1,0 +1,170 @@
+"""Seeded synthetic set-ups of the benchmark configurations, as plain numpy arrays.
+
+Each builder returns a :class:`Setup`; :func:`apply` loads it into any object with the
+reference's ``Simulation`` API (the CUDA one here, or a CPU checker), so the GPU run and its
+comparison run start from identical host arrays.
+
+* ``kelvin_helmholtz``: D2Q9 BGK, fully periodic shear layer (256x256, tau 0.55).
+* ``cylinder_channel``: D2Q9 TRT channel with bounce-back walls, a bounce-back cylinder, fixed
+  inflow/outflow columns and a Boussinesq-coupled D2Q5 tracer (4096x2048, Re 10,000 on the
+  cylinder diameter).
+* ``taylor_green_3d``: D3Q27 periodic Taylor-Green vortex (256^3, Re 1600).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+WALL, FIXED_FLUID, FIXED_SCALAR = 1, 6, 8
+
+
+@dataclass
+class Setup:
+    name: str
+    counts: list[int]
+    collision: str  # "bgk" or "trt"
+    tau: float
+    flags: np.ndarray
+    rho: np.ndarray
+    vel: np.ndarray
+    tracers: list[tuple[str, float, np.ndarray]] = field(default_factory=list)  # name, tau, C
+    gravity: list[float] | None = None
+    couplings: list[tuple[str, float, float, list[float]]] = field(default_factory=list)
+    params: dict = field(default_factory=dict)
+
+    @property
+    def cells(self) -> int:
+        return int(np.prod(self.counts))
+
+
+def kelvin_helmholtz(nx: int = 256, ny: int = 256, tau: float = 0.55, seed: int = 0) -> Setup:
+    """u_x = 0.05 tanh((y - ny/4)/4) below ny/2 and 0.05 tanh((3ny/4 - y)/4) above,
+    u_y = 1e-3 sin(2 pi x / nx) + U(-1e-4, 1e-4); rho = 1."""
+    rng = np.random.default_rng(seed)
+    y = np.arange(ny, dtype=np.float64)[None, :]
+    x = np.arange(nx, dtype=np.float64)[:, None]
+    ux = np.where(y < ny / 2, 0.05 * np.tanh((y - ny / 4) / 4), 0.05 * np.tanh((3 * ny / 4 - y) / 4))
+    ux = np.broadcast_to(ux, (nx, ny))
+    uy = 1e-3 * np.sin(2 * np.pi * x / nx) + rng.uniform(-1e-4, 1e-4, (nx, ny))
+    vel = np.stack([ux, uy], axis=-1).astype(np.float32)
+    return Setup(
+        "kelvin_helmholtz",
+        [nx, ny],
+        "bgk",
+        tau,
+        np.zeros((nx, ny), np.int32),
+        np.ones((nx, ny), np.float32),
+        vel,
+        params={"u0": 0.05},
+    )
+
+
+def cylinder_channel(
+    nx: int = 4096,
+    ny: int = 2048,
+    radius: float = 64.0,
+    u_in: float = 0.05,
+    re: float = 10_000.0,
+    diffusivity: float = 1e-3,
+    buoyancy: float = 1e-5,
+    seed: int = 0,
+) -> Setup:
+    """Channel flow past a cylinder with a buoyant tracer.
+
+    Bounce-back rows at y = 0 and y = ny-1, a bounce-back disc of ``radius`` at (nx/4, ny/2),
+    fixed-velocity (and fixed-tracer) columns at x = 0 and x = nx-1 holding u = (u_in, 0).
+    nu = u_in * 2 radius / re, tau = 3 nu + 1/2 (TRT, magic 1/4). The D2Q5 tracer has
+    tau = 3 D + 1/2 and starts as a seeded random 0/1 band across the middle third of the
+    channel height; it couples back with acc = g * alpha * C, alpha g = buoyancy * (0, -1).
+    """
+    rng = np.random.default_rng(seed)
+    nu = u_in * 2 * radius / re
+    tau = 3 * nu + 0.5
+    flags = np.zeros((nx, ny), np.int32)
+    flags[:, 0] = WALL
+    flags[:, -1] = WALL
+    x = np.arange(nx)[:, None]
+    y = np.arange(ny)[None, :]
+    cx, cy = nx // 4, ny // 2
+    flags[(x - cx) ** 2 + (y - cy) ** 2 <= radius**2] = WALL
+    flags[0, 1:-1] = FIXED_FLUID | FIXED_SCALAR
+    flags[-1, 1:-1] = FIXED_FLUID | FIXED_SCALAR
+    vel = np.zeros((nx, ny, 2), np.float32)
+    vel[..., 0] = u_in
+    vel[flags == WALL] = 0.0
+    rho = np.ones((nx, ny), np.float32)
+    band = np.zeros((nx, ny), np.float32)
+    lo, hi = ny // 3, 2 * ny // 3
+    band[:, lo:hi] = (rng.uniform(size=(nx, hi - lo)) < 0.5).astype(np.float32)
+    band[0, :] = 0.0
+    band[-1, :] = 0.0
+    tau_g = 3 * diffusivity + 0.5
+    return Setup(
+        "cylinder_channel",
+        [nx, ny],
+        "trt",
+        tau,
+        flags,
+        rho,
+        vel,
+        tracers=[("tracer", tau_g, band)],
+        couplings=[("tracer", 1.0, 0.0, [0.0, -buoyancy])],
+        params={"radius": radius, "u_in": u_in, "re": re, "nu": nu, "diffusivity": diffusivity},
+    )
+
+
+def taylor_green_3d(n: int = 256, u0: float = 0.05, re: float = 1600.0) -> Setup:
+    """u = u0 (sin kx cos ky cos kz, -cos kx sin ky cos kz, 0), k = 2 pi / n, with the pressure
+    field in rho = 1 + 3 p, p = u0^2/16 (cos 2kx + cos 2ky)(cos 2kz + 2);
+    nu = u0 (n / 2 pi) / re, tau = 3 nu + 1/2."""
+    k = 2 * math.pi / n
+    c = np.arange(n, dtype=np.float64)
+    X, Y, Z = np.meshgrid(c, c, c, indexing="ij")
+    vel = np.empty((n, n, n, 3), np.float32)
+    vel[..., 0] = u0 * np.sin(k * X) * np.cos(k * Y) * np.cos(k * Z)
+    vel[..., 1] = -u0 * np.cos(k * X) * np.sin(k * Y) * np.cos(k * Z)
+    vel[..., 2] = 0.0
+    p = u0**2 / 16 * (np.cos(2 * k * X) + np.cos(2 * k * Y)) * (np.cos(2 * k * Z) + 2)
+    rho = (1.0 + 3.0 * p).astype(np.float32)
+    nu = u0 * (n / (2 * math.pi)) / re
+    return Setup(
+        "taylor_green_3d",
+        [n, n, n],
+        "bgk",
+        3 * nu + 0.5,
+        np.zeros((n, n, n), np.int32),
+        rho,
+        vel,
+        params={"u0": u0, "re": re, "nu": nu},
+    )
+
+
+def apply(sim, setup: Setup, omega_for, tracer_handle=None) -> None:
+    """Loads ``setup`` into a Simulation-like object.
+
+    ``omega_for(kind, tau)`` builds the collision parameters of that object's API.
+    ``tracer_handle(sim, name, omega)`` adds a tracer and returns (handle, val array);
+    by default the reference API ``sim.add_tracer(name, omega).val`` is used.
+    """
+    flags = sim.cells.flags if hasattr(sim, "cells") else sim.flags
+    rho = sim.fluid.rho if hasattr(sim, "fluid") else sim.rho
+    vel = sim.fluid.vel if hasattr(sim, "fluid") else sim.vel
+    flags[...] = setup.flags
+    rho[...] = setup.rho
+    vel[...] = setup.vel
+    handles = {}
+    for name, tau_t, val in setup.tracers:
+        if tracer_handle is None:
+            h = sim.add_tracer(name, omega_for("bgk", tau_t))
+            h.val[...] = val
+        else:
+            h, arr = tracer_handle(sim, name, omega_for("bgk", tau_t))
+            arr[...] = val
+        handles[name] = h
+    if setup.gravity is not None:
+        sim.set_gravity(np.asarray(setup.gravity, np.float32))
+    for name, alpha, c0, g in setup.couplings:
+        sim.add_boussinesq_coupling(handles[name], alpha, c0, np.asarray(g, np.float32))

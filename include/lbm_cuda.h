@@ -1,0 +1,155 @@
+/*
+ * lbm_cuda.h -- C ABI of the CUDA (sm_100a) lattice-Boltzmann backend.
+ *
+ * This is the device layer that replaces the OpenCL backend of djbarker/boltzmann
+ * (src/opencl.rs, plus the enqueue calls of src/simulation.rs and src/fields.rs). A host layer
+ * (the Python extension boltzmann_b200.boltzmann here; pyo3 bindings wherever Rust is available)
+ * owns the host arrays, keeps the reference's semantics (upload at the first iterate call,
+ * read-back after every call) and calls these functions.
+ *
+ * Conventions
+ *   - Every function returns LBM_OK (0) or an lbm_status; lbm_last_error() then describes the
+ *     failure (thread-local). No C++ exception crosses this boundary.
+ *   - Host arrays use the reference's host layouts (row-major, x slowest):
+ *       flags int32 [N], rho float [N], vel float [N, dim], tracer val float [N],
+ *       populations float [N, q] (checkpoint layout, src/fields.rs:71-75),
+ *     where N = counts[0] * ... * counts[dim-1].
+ *   - All device work of one simulation runs on its own CUDA stream; functions that return
+ *     host data synchronise that stream first.
+ *   - The device layout is internal: populations structure-of-arrays, optionally stored as
+ *     16-bit offsets from the lattice weights (LBM_STORAGE_F16 / _BF16).
+ */
+#ifndef LBM_CUDA_H
+#define LBM_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define LBM_API __attribute__((visibility("default")))
+#else
+#define LBM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct lbm_sim lbm_sim;
+
+enum lbm_status {
+  LBM_OK = 0,
+  LBM_ERR_ARGUMENT = 1,    /* bad argument (odd iters, unknown model, wrong index, ...) */
+  LBM_ERR_UNSUPPORTED = 2, /* no kernel for this combination ("Kernel not found") */
+  LBM_ERR_CUDA = 3,        /* a CUDA runtime call failed */
+  LBM_ERR_STATE = 4        /* call not valid in the current state */
+};
+
+enum lbm_collision { LBM_BGK = 0, LBM_TRT = 1 };
+
+enum lbm_storage {
+  LBM_STORAGE_F32 = 0,  /* float populations (the reference's precision) */
+  LBM_STORAGE_F16 = 1,  /* half offsets f_i - w_i, collision in float */
+  LBM_STORAGE_BF16 = 2, /* bfloat16 offsets f_i - w_i, collision in float */
+  LBM_STORAGE_F64 = 3   /* double populations and arithmetic (the FP64 comparison run) */
+};
+
+/* Thread-local description of the last failure. */
+LBM_API const char* lbm_last_error(void);
+
+/* ABI version of this header (bumped on any signature change). */
+LBM_API int lbm_abi_version(void);
+
+/* Creates a simulation on the current CUDA device: flags = 0, rho = 1, vel = 0, populations 0.
+ * Replaces OpenCLCtx::new + Simulation::new + Fluid::new
+ * (src/opencl.rs:102-171, src/simulation.rs:179-192, src/fields.rs:68-82).
+ * dim in {1,2,3}; q must name a velocity set of src/velocities.rs:55-64 (else
+ * LBM_ERR_ARGUMENT, "Unknown model"); a set without an update kernel is accepted here and
+ * rejected by lbm_iterate, as in the reference. */
+LBM_API int lbm_create(int dim, const int64_t* counts, int q, int collision, float omega_pos,
+               float omega_neg, int storage, lbm_sim** out);
+
+/* Releases all device memory of the simulation. */
+LBM_API int lbm_destroy(lbm_sim* sim);
+
+/* "<device name> GPU", the analogue of Simulation.device_info (src/lib.rs:205-215). */
+LBM_API int lbm_device_info(lbm_sim* sim, char* buf, int len);
+
+/* Device bytes held by populations, rho, vel and tracers (src/lib.rs:228-236 counts host
+ * mirrors of the same arrays). */
+LBM_API int lbm_device_bytes(lbm_sim* sim, int64_t* out);
+
+/* Adds an advection-diffusion tracer (g = 0, val = 0) and returns its index.
+ * Replaces Scalar::new + Simulation::add_tracer (src/fields.rs:152-163,
+ * src/simulation.rs:221-229). */
+LBM_API int lbm_add_tracer(lbm_sim* sim, int q, int collision, float omega_pos, float omega_neg,
+                   int* out_index);
+
+/* Constant body force, dim floats (src/simulation.rs:194-196). */
+LBM_API int lbm_set_gravity(lbm_sim* sim, const float* g);
+
+/* Boussinesq coupling acc = g * alpha * (C - c0) to tracer `tracer`, dim floats of g
+ * (src/simulation.rs:201-216). With several couplings the last one added sets the
+ * acceleration, and any coupling overrides the constant body force, as in
+ * src/simulation.rs:326-373. */
+LBM_API int lbm_add_coupling(lbm_sim* sim, int tracer, float alpha, float c0, const float* g);
+
+/* Host -> device copies of the macroscopic fields (Data::enqueue_write, src/opencl.rs:253-265,
+ * as called by Simulation::finalize, src/simulation.rs:254-275). */
+LBM_API int lbm_upload_flags(lbm_sim* sim, const int32_t* flags);
+LBM_API int lbm_upload_fluid(lbm_sim* sim, const float* rho, const float* vel);
+LBM_API int lbm_upload_tracer(lbm_sim* sim, int tracer, const float* val);
+
+/* f = feq(rho, vel) and every tracer's g = feq(val, vel) on the device, bit-identical in FP32 to
+ * Fluid::equilibrate / Scalar::equilibrate (src/fields.rs:106-114, 185-193,
+ * src/velocities.rs:43-52). */
+LBM_API int lbm_equilibrate(lbm_sim* sim);
+
+/* Same for one tracer only, against the fluid velocity currently on the device. Used for a
+ * tracer added after the first iterate call, whose device buffers the reference leaves
+ * unwritten (src/simulation.rs:221-229 allocates, only finalize() at iteration 0 uploads). */
+LBM_API int lbm_equilibrate_tracer(lbm_sim* sim, int tracer);
+
+/* Populations in the checkpoint layout float [N, q] (src/simulation.rs:448-479). */
+LBM_API int lbm_upload_f(lbm_sim* sim, const float* f);
+LBM_API int lbm_download_f(lbm_sim* sim, float* f);
+LBM_API int lbm_upload_g(lbm_sim* sim, int tracer, const float* g);
+LBM_API int lbm_download_g(lbm_sim* sim, int tracer, float* g);
+
+/* Advances `iters` AA steps (the per-step loop of Simulation::iterate,
+ * src/simulation.rs:288-433). iters must be even (src/simulation.rs:279-281). Asynchronous:
+ * returns once the steps are enqueued on the simulation's stream. */
+LBM_API int lbm_iterate(lbm_sim* sim, int64_t iters);
+
+/* Device -> host copies after an iterate call (Fluid/Scalar::read_to_host,
+ * src/fields.rs:97-104, 177-183). Synchronous. */
+LBM_API int lbm_download_fluid(lbm_sim* sim, float* rho, float* vel);
+LBM_API int lbm_download_tracer(lbm_sim* sim, int tracer, float* val);
+
+/* Same for an LBM_STORAGE_F64 simulation, in double. */
+LBM_API int lbm_download_fluid_f64(lbm_sim* sim, double* rho, double* vel);
+
+/* FP64 sums over every population slot: out[0] = sum f, out[1..dim] = sum c_i f_i, then one
+ * sum of g per tracer. No reference counterpart (conservation diagnostics). Synchronous. */
+LBM_API int lbm_conservation(lbm_sim* sim, double* out, int len);
+
+/* Sets *out to 1 when a non-finite density was produced by a step that ended an iterate call
+ * since the last query, else 0; clears the flag. The device-side analogue of run_sim's NaN check
+ * (python/boltzmann/simulation.py:241-242). Synchronous. */
+LBM_API int lbm_nonfinite(lbm_sim* sim, int* out);
+
+/* Blocks until all work of the simulation is done. */
+LBM_API int lbm_synchronize(lbm_sim* sim);
+
+/* The simulation's cudaStream_t, for callers that time or order work around it. */
+LBM_API int lbm_stream(lbm_sim* sim, void** stream);
+
+/* Page-locked host memory for host arrays (fast transfers); NULL on failure. */
+LBM_API void* lbm_host_alloc(size_t bytes);
+LBM_API void lbm_host_free(void* ptr);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBM_CUDA_H */
