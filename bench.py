@@ -143,17 +143,18 @@ class ClockSampler:
         }
 
 
-def omega_for(kind: str, tau: float):
+def omega_for(kind: str, tau: float, tau_neg: float | None = None):
     from boltzmann_b200.core import bgk, trt
 
-    return bgk(tau) if kind == "bgk" else trt(tau)
+    return bgk(tau) if kind == "bgk" else trt(tau, tau_neg)
 
 
 def build_sim(setup, storage: str):
     from boltzmann_b200 import workloads
     from boltzmann_b200.core import Simulation
 
-    sim = Simulation("gpu", setup.counts, omega_for(setup.collision, setup.tau), storage=storage)
+    sim = Simulation("gpu", setup.counts, omega_for(setup.collision, setup.tau, setup.tau_neg),
+                     storage=storage)
     workloads.apply(sim, setup, omega_for)
     return sim
 
@@ -168,11 +169,11 @@ def cpu_reference_rate(setup, budget_s: float, max_pairs: int | None = None) -> 
     kind = "reference" if reference_available() else "port"
     threads = default_threads()
 
-    def om(k, tau):
-        return Omega.bgk(tau) if k == "bgk" else Omega.trt(tau)
+    def om(k, tau, tau_neg=None):
+        return Omega.bgk(tau) if k == "bgk" else Omega.trt(tau, tau_neg)
 
-    sim = OracleSimulation(setup.counts, om(setup.collision, setup.tau), backend=kind,
-                           nthreads=threads)
+    sim = OracleSimulation(setup.counts, om(setup.collision, setup.tau, setup.tau_neg),
+                           backend=kind, nthreads=threads)
 
     def tracer_handle(s, name, o):
         return name, s.add_tracer(name, o).val

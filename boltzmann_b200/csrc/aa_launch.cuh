@@ -2,6 +2,10 @@
 // lattice so the instantiations compile in parallel.
 #pragma once
 
+#include <atomic>
+#include <mutex>
+
+#include "aa_pipe.cuh"
 #include "aa_step.cuh"
 #include "sim.h"
 
@@ -59,25 +63,70 @@ void step_geometry(const StepArgs<Real>& a, dim3& grid, dim3& block) {
   grid = dim3((a.nz + bx - 1) / bx, a.ny < 65535 ? a.ny : 65535, a.nx < 65535 ? a.nx : 65535);
 }
 
+// Pipeline depth: enough stages to cover DRAM latency within the shared memory of 2-3 CTAs per
+// SM (D2Q9 + D2Q5 F32: 64 KB per 256-thread CTA; D3Q27 F32: 89 KB; D3Q27 F64: 119 KB).
+template <class L, int K>
+constexpr int pipe_stages() {
+  return L::Q > 9 ? (sizeof(typename Pop<K>::type) == 8 ? 2 : 3) : 4;
+}
+
+template <class L, bool TRT, int K, bool EVEN, int NT>
+cudaError_t launch_one(const StepArgs<typename Pop<K>::real>& a, cudaStream_t stream) {
+  if constexpr (sizeof(typename Pop<K>::type) == 2) {
+    dim3 grid, block;
+    step_geometry(a, grid, block);
+    aa_step_kernel<L, TRT, K, EVEN, NT><<<grid, block, 0, stream>>>(a);
+    return cudaGetLastError();
+  } else {
+    constexpr int S = pipe_stages<L, K>();
+    auto kern = aa_pipe_kernel<L, TRT, K, EVEN, NT, S>;
+    const int threads = a.nz >= 256 ? 256 : ((a.nz + 31) / 32) * 32;
+    const size_t smem = pipe_smem_bytes<L, K, NT, S>(threads);
+    static std::once_flag attr_once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(attr_once, [&] {
+      attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)pipe_smem_bytes<L, K, NT, S>(256));
+    });
+    if (attr_err != cudaSuccess) return attr_err;
+    // Resident CTAs per SM for this block size, cached per instantiation.
+    static std::atomic<int> cached_threads{0}, cached_blocks{0};
+    int per_sm = cached_threads.load() == threads ? cached_blocks.load() : 0;
+    if (per_sm == 0) {
+      cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+      if (e != cudaSuccess) return e;
+      if (per_sm < 1) per_sm = 1;
+      cached_blocks.store(per_sm);
+      cached_threads.store(threads);
+    }
+    int device = 0, sms = 148;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const int gx = (a.nz + threads - 1) / threads;
+    const long long rows = (long long)a.nx * a.ny;
+    long long gy = ((long long)sms * per_sm + gx - 1) / gx;
+    if (gy > rows) gy = rows;
+    if (gy > 65535) gy = 65535;
+    if (gy < 1) gy = 1;
+    kern<<<dim3(gx, (unsigned)gy, 1), threads, smem, stream>>>(a);
+    return cudaGetLastError();
+  }
+}
+
 template <class L, bool TRT, int K>
 cudaError_t launch_typed(const lbm_sim& s, bool even, bool write_moments) {
   using Real = typename Pop<K>::real;
   const StepArgs<Real> a = make_step_args<Real>(s, write_moments);
-  dim3 grid, block;
-  step_geometry(a, grid, block);
-  const bool tracers = a.ntracers > 0;
+  // Fused tracers: none, exactly one (loads hoisted with the fluid's), or a runtime count.
+  const int nt = a.ntracers;
   if (even) {
-    if (tracers)
-      aa_step_kernel<L, TRT, K, true, true><<<grid, block, 0, s.stream>>>(a);
-    else
-      aa_step_kernel<L, TRT, K, true, false><<<grid, block, 0, s.stream>>>(a);
-  } else {
-    if (tracers)
-      aa_step_kernel<L, TRT, K, false, true><<<grid, block, 0, s.stream>>>(a);
-    else
-      aa_step_kernel<L, TRT, K, false, false><<<grid, block, 0, s.stream>>>(a);
+    if (nt == 0) return launch_one<L, TRT, K, true, 0>(a, s.stream);
+    if (nt == 1) return launch_one<L, TRT, K, true, 1>(a, s.stream);
+    return launch_one<L, TRT, K, true, -1>(a, s.stream);
   }
-  return cudaGetLastError();
+  if (nt == 0) return launch_one<L, TRT, K, false, 0>(a, s.stream);
+  if (nt == 1) return launch_one<L, TRT, K, false, 1>(a, s.stream);
+  return launch_one<L, TRT, K, false, -1>(a, s.stream);
 }
 
 template <class L>

@@ -95,46 +95,66 @@ struct CellPos {
   }
 };
 
-// AA load of one velocity set's populations for this cell.
-template <class L, class P, bool EVEN>
+// AA load of one velocity set's populations for this cell: deviations d_i = f_i - W_i when DEV,
+// full values otherwise.
+template <class L, class P, bool EVEN, bool DEV>
 __device__ __forceinline__ void aa_load(const typename P::type* __restrict__ f, long long n,
                                         const CellPos& c, typename P::real (&v)[L::Q]) {
   using Real = typename P::real;
 #pragma unroll
   for (int i = 0; i < L::Q; ++i) {
-    if constexpr (EVEN)
-      v[i] = P::load(f + (long long)i * n + c.upstream<L>(i), weight<L, Real>(i));
+    const typename P::type* p =
+        EVEN ? f + (long long)i * n + c.upstream<L>(i) : f + (long long)opp(i) * n + c.cell;
+    // Slot i (even) and slot opp(i) (odd) share the weight of direction i.
+    if constexpr (DEV)
+      v[i] = P::load_dev(p, weight<L, Real>(i));
     else
-      v[i] = P::load(f + (long long)opp(i) * n + c.cell, weight<L, Real>(i));
+      v[i] = P::load(p, weight<L, Real>(i));
   }
 }
 
 // AA store matching aa_load.
-template <class L, class P, bool EVEN>
+template <class L, class P, bool EVEN, bool DEV>
 __device__ __forceinline__ void aa_store(typename P::type* __restrict__ f, long long n,
                                          const CellPos& c, const typename P::real (&v)[L::Q]) {
   using Real = typename P::real;
 #pragma unroll
   for (int i = 0; i < L::Q; ++i) {
-    if constexpr (EVEN)
-      P::store(f + (long long)i * n + c.upstream<L>(i), v[opp(i)], weight<L, Real>(i));
+    typename P::type* p = f + (long long)i * n + (EVEN ? c.upstream<L>(i) : c.cell);
+    const Real val = EVEN ? v[opp(i)] : v[i];
+    if constexpr (DEV)
+      P::store_dev(p, val, weight<L, Real>(i));
     else
-      P::store(f + (long long)i * n + c.cell, v[i], weight<L, Real>(i));
+      P::store(p, val, weight<L, Real>(i));
   }
 }
 
 // BGK or TRT collision against the second-order equilibrium
 //   feq_i = w_i r (1 + 3 c_i.u + 4.5 (c_i.u)^2 - 1.5 u.u),
-// evaluated per opposite pair (i, i+1): feq = A +- B with A = w r (1 + 4.5 cu^2 - 1.5 uu) and
-// B = 3 w r cu. TRT relaxes the symmetric part with om_pos and the antisymmetric part with
-// om_neg (src/lib.cl:697-719); BGK relaxes both with om_pos (src/lib.cl:266-274).
-template <class L, bool TRT, class Real>
-__device__ __forceinline__ void collide(Real (&f)[L::Q], Real r, const Real (&u)[3], Real uu,
-                                        Real om_pos, Real om_neg) {
-  const Real base = Real(1) - Real(1.5) * uu;
+// evaluated per opposite pair (i, i+1) as feq = A +- B (symmetric and antisymmetric parts).
+// TRT relaxes the symmetric part with om_pos and the antisymmetric part with om_neg
+// (src/lib.cl:697-719); BGK relaxes both with om_pos (src/lib.cl:266-274).
+//
+// DEV: v holds deviations d_i = f_i - W_i and dr = r - 1, and the equilibrium is formed as
+// the deviation e_i = feq_i - W_i = w_i r X_i + (w_i dr + (w_i - W_i)),
+// X_i = 3cu + 4.5cu^2 - 1.5uu. Every term is small, so the stored f_i = W_i + d_i carries about
+// one rounding, like the reference's double-precision update. The constant w_i - W_i (below one
+// ulp of e_i) is added to the small w_i dr term first: added last it would be rounded away in
+// the same direction every step, a mass drift of ~4e-9 per cell and step.
+// Otherwise v holds full values (the tracers, whose concentration is not near a fixed offset).
+// The weights enter as exact integers k_i times r / kDen (one unbiased rounding per cell):
+// float-rounded weights do not sum to one (D2Q9: 1 + 7.5e-9), which would otherwise add a
+// systematic mass and momentum drift of that size per step.
+template <class L, bool TRT, bool DEV, class Real>
+__device__ __forceinline__ void collide(Real (&v)[L::Q], Real r, Real dr, const Real (&u)[3],
+                                        Real uu, Real om_pos, Real om_neg) {
+  const Real ru = r / Real(L::kDen);
+  const Real unit = DEV ? dr / Real(L::kDen) : ru;  // the w_i (r or dr) term per unit weight
+  const Real quad = Real(-1.5) * uu;
   {
-    const Real a0 = weight<L, Real>(0) * r * base;
-    f[0] += om_pos * (a0 - f[0]);
+    const Real k0 = Real(L::wk(0));
+    const Real e0 = k0 * ru * quad + (k0 * unit + (DEV ? weight_gap<L, Real>(0) : Real(0)));
+    v[0] += om_pos * (e0 - v[0]);
   }
 #pragma unroll
   for (int i = 1; i < L::Q; i += 2) {
@@ -144,26 +164,75 @@ __device__ __forceinline__ void collide(Real (&f)[L::Q], Real r, const Real (&u)
       if (comp<L>(i, a) > 0) cu += u[a];
       if (comp<L>(i, a) < 0) cu -= u[a];
     }
-    const Real wr = weight<L, Real>(i) * r;
-    const Real A = wr * (base + Real(4.5) * cu * cu);
-    const Real B = wr * Real(3) * cu;
+    const Real k = Real(L::wk(i));
+    const Real A =
+        k * ru * (quad + Real(4.5) * cu * cu) + (k * unit + (DEV ? weight_gap<L, Real>(i) : Real(0)));
+    const Real B = k * ru * Real(3) * cu;
     if constexpr (TRT) {
-      const Real s = Real(0.5) * (f[i] + f[i + 1]);
-      const Real d = Real(0.5) * (f[i] - f[i + 1]);
+      const Real s = Real(0.5) * (v[i] + v[i + 1]);
+      const Real d = Real(0.5) * (v[i] - v[i + 1]);
       const Real fp = om_pos * (A - s);
       const Real fn = om_neg * (B - d);
-      f[i] += fp + fn;
-      f[i + 1] += fp - fn;
+      v[i] += fp + fn;
+      v[i + 1] += fp - fn;
     } else {
-      f[i] += om_pos * (A + B - f[i]);
-      f[i + 1] += om_pos * (A - B - f[i + 1]);
+      v[i] += om_pos * (A + B - v[i]);
+      v[i + 1] += om_pos * (A - B - v[i + 1]);
     }
   }
 }
 
-template <class L, bool TRT, int K, bool EVEN, bool TRACERS>
-__global__ void __launch_bounds__(256)
-    aa_step_kernel(const __grid_constant__ StepArgs<typename Pop<K>::real> a) {
+// Advection-diffusion update of one tracer cell in the fluid velocity u just computed
+// (src/lib.cl:102-189, 303-405), with its populations already loaded into g.
+template <class TL, class TP, bool EVEN, class Real>
+__device__ __forceinline__ void tracer_update(const TracerArgs<Real>& tr, long long n,
+                                              const CellPos& c, int flag, Real (&g)[TL::Q],
+                                              const Real (&u)[3], Real uu, bool keep) {
+  Real rt = 0;
+#pragma unroll
+  for (int i = 0; i < TL::Q; ++i) rt += g[i];
+  Real om = tr.omega;
+  const bool tfixed = (flag & 8) != 0;  // FIXED_SCALAR_VALUE (src/lib.cl:156-161)
+  if (tfixed) {
+    om = 1;
+    rt = tr.val[c.cell];
+  }
+  collide<TL, false, false>(g, rt, rt, u, uu, om, om);
+  aa_store<TL, TP, EVEN, false>(tr.g, n, c, g);
+  if (keep && !tfixed) tr.val[c.cell] = rt;
+}
+
+template <class Real>
+__device__ __forceinline__ CellPos make_cellpos(const StepArgs<Real>& a, int x, int y, int z,
+                                                bool neighbours) {
+  CellPos c;
+  c.nx = a.nx;
+  c.ny = a.ny;
+  c.nz = a.nz;
+  c.x = x;
+  c.y = y;
+  c.z = z;
+  c.cell = ((long long)x * a.ny + y) * a.nz + z;
+  if (neighbours) {
+    c.xm = x == 0 ? a.nx - 1 : x - 1;
+    c.xp = x == a.nx - 1 ? 0 : x + 1;
+    c.ym = y == 0 ? a.ny - 1 : y - 1;
+    c.yp = y == a.ny - 1 ? 0 : y + 1;
+    c.zm = z == 0 ? a.nz - 1 : z - 1;
+    c.zp = z == a.nz - 1 ? 0 : z + 1;
+  }
+  return c;
+}
+
+// Everything after the loads for one cell: moments, forcing, fixed-cell override, collision,
+// AA store, end-of-call moments and the fused tracers. f holds the full population values of
+// the AA load, g the first tracer's (NT == 1), cval the coupled tracer's previous value.
+template <class L, bool TRT, int K, bool EVEN, int NT>
+__device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real>& a,
+                                            const CellPos& c, int flag,
+                                            typename Pop<K>::real (&f)[L::Q],
+                                            typename Pop<K>::real (&g)[NT == 1 ? TracerLattice<L::D>::type::Q : 1],
+                                            typename Pop<K>::real cval) {
   using P = Pop<K>;
   using Real = typename P::real;
   using T = typename P::type;
@@ -171,105 +240,100 @@ __global__ void __launch_bounds__(256)
   using TP = Pop<(sizeof(Real) == 8 ? kF64 : kF32)>;
   constexpr int Q = L::Q;
 
+  if (flag & 1) return;  // WALL: never updated (src/lib.cl:210-213)
+
+  // Moments from the full values, summed in slot order as the reference does
+  // (src/lib.cl:249-251).
+  Real r = 0;
+#pragma unroll
+  for (int i = 0; i < Q; ++i) r += f[i];
+  Real u[3] = {0, 0, 0};
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      if (comp<L>(i, ax) > 0) u[ax] += f[i];
+      if (comp<L>(i, ax) < 0) u[ax] -= f[i];
+    }
+  }
+#pragma unroll
+  for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] = u[ax] / r;
+
+  Real om_pos = a.om_pos, om_neg = a.om_neg;
+  // Force as a velocity shift acc / omega (src/lib.cl:253-256; TRT: omega+, 682-685).
+  if (a.acc_mode == kAccConstant) {
+#pragma unroll
+    for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] += a.acc[ax] / om_pos;
+  } else if (a.acc_mode == kAccBoussinesq) {
+    const Real b = a.alpha * (cval - a.c0);
+#pragma unroll
+    for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] += (a.acc[ax] * b) / om_pos;
+  }
+  const bool fixed = (flag & 6) != 0;  // FIXED_FLUID_VELOCITY | FIXED_FLUID_DENSITY
+  if (fixed) {                         // src/lib.cl:257-262
+    om_pos = 1;
+    om_neg = 1;
+    r = a.rho[c.cell];
+#pragma unroll
+    for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] = a.vel[c.cell * L::D + ax - (3 - L::D)];
+  }
+  Real uu = 0;
+#pragma unroll
+  for (int ax = 3 - L::D; ax < 3; ++ax) uu += u[ax] * u[ax];
+
+  // Collide on the deviations d_i = f_i - W_i (exact for values near W_i).
+#pragma unroll
+  for (int i = 0; i < Q; ++i) f[i] -= weight<L, Real>(i);
+  collide<L, TRT, true>(f, r, r - Real(1), u, uu, om_pos, om_neg);
+  aa_store<L, P, EVEN, true>(static_cast<T*>(a.f), a.n, c, f);
+
+  if (a.write_moments && !fixed) {
+    a.rho[c.cell] = r;
+#pragma unroll
+    for (int ax = 3 - L::D; ax < 3; ++ax) a.vel[c.cell * L::D + ax - (3 - L::D)] = u[ax];
+    if (!isfinite(r)) atomicOr(a.status, 1);
+  }
+
+  if constexpr (NT == 1) {
+    const bool keep = a.write_moments || (a.acc_mode == kAccBoussinesq && a.coupled == 0);
+    tracer_update<TL, TP, EVEN>(a.tr[0], a.n, c, flag, g, u, uu, keep);
+  } else if constexpr (NT < 0) {
+    for (int t = 0; t < a.ntracers; ++t) {
+      Real gt[TL::Q];
+      aa_load<TL, TP, EVEN, false>(a.tr[t].g, a.n, c, gt);
+      const bool keep = a.write_moments || (a.acc_mode == kAccBoussinesq && t == a.coupled);
+      tracer_update<TL, TP, EVEN>(a.tr[t], a.n, c, flag, gt, u, uu, keep);
+    }
+  }
+}
+
+// Direct variant: one cell per thread and grid row, loads straight into registers.
+// NT: number of fused tracers known at compile time (0 or 1), or -1 for a runtime count.
+// Every load a cell needs is issued before the first branch on any loaded value, so each thread
+// has one memory phase (walls load populations they then ignore; they are a small fraction).
+template <class L, bool TRT, int K, bool EVEN, int NT>
+__global__ void __launch_bounds__(256)
+    aa_step_kernel(const __grid_constant__ StepArgs<typename Pop<K>::real> a) {
+  using P = Pop<K>;
+  using Real = typename P::real;
+  using T = typename P::type;
+  using TL = typename TracerLattice<L::D>::type;
+  using TP = Pop<(sizeof(Real) == 8 ? kF64 : kF32)>;
+
   const int z = blockIdx.x * blockDim.x + threadIdx.x;
   if (z >= a.nz) return;
 
   for (int x = blockIdx.z; x < a.nx; x += gridDim.z) {
     for (int y = blockIdx.y; y < a.ny; y += gridDim.y) {
-      CellPos c;
-      c.nx = a.nx;
-      c.ny = a.ny;
-      c.nz = a.nz;
-      c.x = x;
-      c.y = y;
-      c.z = z;
-      c.cell = ((long long)x * a.ny + y) * a.nz + z;
-
+      const CellPos c = make_cellpos(a, x, y, z, EVEN);
       const int flag = a.flags[c.cell];
-      if (flag & 1) continue;  // WALL: never updated (src/lib.cl:210-213)
-
-      if constexpr (EVEN) {
-        c.xm = x == 0 ? a.nx - 1 : x - 1;
-        c.xp = x == a.nx - 1 ? 0 : x + 1;
-        c.ym = y == 0 ? a.ny - 1 : y - 1;
-        c.yp = y == a.ny - 1 ? 0 : y + 1;
-        c.zm = z == 0 ? a.nz - 1 : z - 1;
-        c.zp = z == a.nz - 1 ? 0 : z + 1;
-      }
-
-      Real f[Q];
-      aa_load<L, P, EVEN>(static_cast<const T*>(a.f), a.n, c, f);
-
-      // Moments (src/lib.cl:249-251).
-      Real r = 0;
-#pragma unroll
-      for (int i = 0; i < Q; ++i) r += f[i];
-      Real u[3] = {0, 0, 0};
-#pragma unroll
-      for (int i = 0; i < Q; ++i) {
-#pragma unroll
-        for (int ax = 0; ax < 3; ++ax) {
-          if (comp<L>(i, ax) > 0) u[ax] += f[i];
-          if (comp<L>(i, ax) < 0) u[ax] -= f[i];
-        }
-      }
-#pragma unroll
-      for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] = u[ax] / r;
-
-      Real om_pos = a.om_pos, om_neg = a.om_neg;
-      // Force as a velocity shift acc / omega (src/lib.cl:253-256; TRT: omega+, 682-685).
-      if (a.acc_mode == kAccConstant) {
-#pragma unroll
-        for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] += a.acc[ax] / om_pos;
-      } else if (a.acc_mode == kAccBoussinesq) {
-        const Real b = a.alpha * (a.coupled_val[c.cell] - a.c0);
-#pragma unroll
-        for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] += (a.acc[ax] * b) / om_pos;
-      }
-      const bool fixed = (flag & 6) != 0;  // FIXED_FLUID_VELOCITY | FIXED_FLUID_DENSITY
-      if (fixed) {                         // src/lib.cl:257-262
-        om_pos = 1;
-        om_neg = 1;
-        r = a.rho[c.cell];
-#pragma unroll
-        for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] = a.vel[c.cell * L::D + ax - (3 - L::D)];
-      }
-      Real uu = 0;
-#pragma unroll
-      for (int ax = 3 - L::D; ax < 3; ++ax) uu += u[ax] * u[ax];
-
-      collide<L, TRT>(f, r, u, uu, om_pos, om_neg);
-      aa_store<L, P, EVEN>(static_cast<T*>(a.f), a.n, c, f);
-
-      if (a.write_moments && !fixed) {
-        a.rho[c.cell] = r;
-#pragma unroll
-        for (int ax = 3 - L::D; ax < 3; ++ax) a.vel[c.cell * L::D + ax - (3 - L::D)] = u[ax];
-        if (!isfinite(r)) atomicOr(a.status, 1);
-      }
-
-      if constexpr (TRACERS) {
-        // Advection-diffusion tracers in the fluid velocity just computed
-        // (src/lib.cl:102-189, 303-405).
-        for (int t = 0; t < a.ntracers; ++t) {
-          const TracerArgs<Real>& tr = a.tr[t];
-          Real g[TL::Q];
-          aa_load<TL, TP, EVEN>(tr.g, a.n, c, g);
-          Real rt = 0;
-#pragma unroll
-          for (int i = 0; i < TL::Q; ++i) rt += g[i];
-          Real om = tr.omega;
-          const bool tfixed = (flag & 8) != 0;  // FIXED_SCALAR_VALUE
-          if (tfixed) {
-            om = 1;
-            rt = tr.val[c.cell];
-          }
-          collide<TL, false>(g, rt, u, uu, om, om);
-          aa_store<TL, TP, EVEN>(tr.g, a.n, c, g);
-          const bool keep = a.write_moments || (a.acc_mode == kAccBoussinesq && t == a.coupled);
-          if (keep && !tfixed) tr.val[c.cell] = rt;
-        }
-      }
+      Real f[L::Q];
+      aa_load<L, P, EVEN, false>(static_cast<const T*>(a.f), a.n, c, f);
+      Real g[NT == 1 ? TL::Q : 1];
+      if constexpr (NT == 1) aa_load<TL, TP, EVEN, false>(a.tr[0].g, a.n, c, g);
+      Real cval = 0;
+      if (a.acc_mode == kAccBoussinesq) cval = a.coupled_val[c.cell];
+      update_cell<L, TRT, K, EVEN, NT>(a, c, flag, f, g, cval);
     }
   }
 }

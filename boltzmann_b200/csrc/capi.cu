@@ -152,7 +152,9 @@ int lbm_create(int dim, const int64_t* counts, int q, int collision, float omega
   if ((e = cudaMalloc(&s->rho, (size_t)n * rb)) != cudaSuccess) return bail(e, "cudaMalloc(rho)");
   if ((e = cudaMalloc(&s->vel, (size_t)n * dim * rb)) != cudaSuccess)
     return bail(e, "cudaMalloc(vel)");
-  if ((e = cudaMalloc((void**)&s->flags, (size_t)n)) != cudaSuccess)
+  // Flags are padded to whole 256-byte blocks: kernels read them as aligned 4-byte words.
+  const size_t flag_bytes = ((size_t)n + 255) / 256 * 256;
+  if ((e = cudaMalloc((void**)&s->flags, flag_bytes)) != cudaSuccess)
     return bail(e, "cudaMalloc(flags)");
   if ((e = cudaMalloc((void**)&s->status, 64 * sizeof(double))) != cudaSuccess)
     return bail(e, "cudaMalloc(status)");
@@ -163,7 +165,7 @@ int lbm_create(int dim, const int64_t* counts, int q, int collision, float omega
   if ((e = cudaMemsetAsync(s->f, 0, (size_t)n * q * lbm::pop_bytes(storage), s->stream)) ||
       (e = lbm::fill_value(s->rho, n, 1.0, storage == LBM_STORAGE_F64, s->stream)) ||
       (e = cudaMemsetAsync(s->vel, 0, (size_t)n * dim * rb, s->stream)) ||
-      (e = cudaMemsetAsync(s->flags, 0, (size_t)n, s->stream)) ||
+      (e = cudaMemsetAsync(s->flags, 0, flag_bytes, s->stream)) ||
       (e = cudaMemsetAsync(s->status, 0, 64 * sizeof(double), s->stream)) ||
       (e = cudaStreamSynchronize(s->stream)))
     return bail(e, "initialise fields");

@@ -89,16 +89,18 @@ cudaError_t equilibrate_storage(int storage, void* f, const void* rho, const voi
   return cudaErrorInvalidValue;
 }
 
+// `storage` is the storage kind of the buffer f (the fluid's kind, or F32/F64 for tracers).
 cudaError_t equilibrate_any(int d, int q, int storage, void* f, const void* rho, const void* vel,
                             int64_t n, cudaStream_t s) {
+  if (d == 1 && q == 3) return equilibrate_storage<D1Q3>(storage, f, rho, vel, n, s);
   if (d == 2 && q == 9) return equilibrate_storage<D2Q9>(storage, f, rho, vel, n, s);
+  if (d == 2 && q == 5) return equilibrate_storage<D2Q5>(storage, f, rho, vel, n, s);
+  if (d == 3 && q == 7) return equilibrate_storage<D3Q7>(storage, f, rho, vel, n, s);
   if (d == 3 && q == 27) return equilibrate_storage<D3Q27>(storage, f, rho, vel, n, s);
-  // Tracer sets are stored in the compute precision (float, or double for F64).
-  const int ts = storage == kF64 ? kF64 : kF32;
-  if (d == 2 && q == 5) return equilibrate_storage<D2Q5>(ts, f, rho, vel, n, s);
-  if (d == 3 && q == 7) return equilibrate_storage<D3Q7>(ts, f, rho, vel, n, s);
   return cudaErrorNotSupported;
 }
+
+inline int tracer_storage(const lbm_sim& sim) { return sim.storage == kF64 ? kF64 : kF32; }
 
 // Per-slot weights of any velocity set, for the offset encodings of the layout transposes.
 struct SlotWeights {
@@ -117,7 +119,8 @@ SlotWeights slot_weights() {
 }
 
 bool weights_for(int d, int q, SlotWeights& out) {
-  if (d == 2 && q == 9) out = slot_weights<D2Q9>();
+  if (d == 1 && q == 3) out = slot_weights<D1Q3>();
+  else if (d == 2 && q == 9) out = slot_weights<D2Q9>();
   else if (d == 3 && q == 27) out = slot_weights<D3Q27>();
   else if (d == 2 && q == 5) out = slot_weights<D2Q5>();
   else if (d == 3 && q == 7) out = slot_weights<D3Q7>();
@@ -230,7 +233,7 @@ cudaError_t equilibrate(const lbm_sim& sim) {
                                   sim.stream);
   if (e != cudaSuccess) return e;
   for (const lbm_sim::Tracer& t : sim.tracers) {
-    e = equilibrate_any(sim.dim, t.q, sim.storage, t.g, t.val, sim.vel, sim.n, sim.stream);
+    e = equilibrate_any(sim.dim, t.q, tracer_storage(sim), t.g, t.val, sim.vel, sim.n, sim.stream);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -238,7 +241,8 @@ cudaError_t equilibrate(const lbm_sim& sim) {
 
 cudaError_t equilibrate_tracer(const lbm_sim& sim, int tracer) {
   const lbm_sim::Tracer& t = sim.tracers[tracer];
-  return equilibrate_any(sim.dim, t.q, sim.storage, t.g, t.val, sim.vel, sim.n, sim.stream);
+  return equilibrate_any(sim.dim, t.q, tracer_storage(sim), t.g, t.val, sim.vel, sim.n,
+                         sim.stream);
 }
 
 cudaError_t populations_from_aos(const lbm_sim& sim, int tracer, const float* d_aos) {
@@ -250,7 +254,7 @@ cudaError_t populations_from_aos(const lbm_sim& sim, int tracer, const float* d_
   }
   const lbm_sim::Tracer& t = sim.tracers[tracer];
   if (!weights_for(sim.dim, t.q, sw)) return cudaErrorNotSupported;
-  return transpose<true>(sim.storage == kF64 ? kF64 : kF32, t.g, const_cast<float*>(d_aos), sim.n,
+  return transpose<true>(tracer_storage(sim), t.g, const_cast<float*>(d_aos), sim.n,
                          t.q, sw, sim.stream);
 }
 
@@ -262,7 +266,7 @@ cudaError_t populations_to_aos(const lbm_sim& sim, int tracer, float* d_aos) {
   }
   const lbm_sim::Tracer& t = sim.tracers[tracer];
   if (!weights_for(sim.dim, t.q, sw)) return cudaErrorNotSupported;
-  return transpose<false>(sim.storage == kF64 ? kF64 : kF32, t.g, d_aos, sim.n, t.q, sw,
+  return transpose<false>(tracer_storage(sim), t.g, d_aos, sim.n, t.q, sw,
                           sim.stream);
 }
 
@@ -293,7 +297,7 @@ cudaError_t conservation_sums(const lbm_sim& sim, double* d_out) {
   for (size_t t = 0; t < sim.tracers.size(); ++t) {
     const lbm_sim::Tracer& tr = sim.tracers[t];
     if (!weights_for(sim.dim, tr.q, sw)) return cudaErrorNotSupported;
-    e = sums(sim.storage == kF64 ? kF64 : kF32, tr.g, sim.n, tr.q, sim.dim, sw,
+    e = sums(tracer_storage(sim), tr.g, sim.n, tr.q, sim.dim, sw,
              d_out + 1 + sim.dim + t, 1, sim.stream);
     if (e != cudaSuccess) return e;
   }

@@ -8,8 +8,24 @@
 
 namespace lbm {
 
+// w(i) / wd(i): the weight in float / double (float is what the reference's host equilibrium
+// uses, src/velocities.rs:73-85). wk(i) / kDen: the same weight as an exact integer multiple of
+// 1 / kDen, used by the collision so that the weights sum to exactly one in any precision.
+
+struct D1Q3 {
+  static constexpr int D = 1, Q = 3, kDen = 6;
+  __host__ __device__ static constexpr int c(int i, int a) {
+    constexpr int t[3][3] = {{0, 0, 0}, {1, 0, 0}, {-1, 0, 0}};
+    return t[i][a];
+  }
+  __host__ __device__ static constexpr int wk(int i) { return i == 0 ? 4 : 1; }
+  __host__ __device__ static constexpr float w(int i) { return i == 0 ? 4.0f / 6.0f : 1.0f / 6.0f; }
+  __host__ __device__ static constexpr double wd(int i) { return i == 0 ? 4.0 / 6.0 : 1.0 / 6.0; }
+};
+
 struct D2Q9 {
-  static constexpr int D = 2, Q = 9;
+  static constexpr int D = 2, Q = 9, kDen = 36;
+  __host__ __device__ static constexpr int wk(int i) { return i == 0 ? 16 : (i < 5 ? 4 : 1); }
   __host__ __device__ static constexpr int c(int i, int a) {
     constexpr int t[9][3] = {{0, 0, 0}, {1, 0, 0},   {-1, 0, 0}, {0, 1, 0}, {0, -1, 0},
                              {1, 1, 0}, {-1, -1, 0}, {1, -1, 0}, {-1, 1, 0}};
@@ -24,7 +40,8 @@ struct D2Q9 {
 };
 
 struct D2Q5 {
-  static constexpr int D = 2, Q = 5;
+  static constexpr int D = 2, Q = 5, kDen = 6;
+  __host__ __device__ static constexpr int wk(int i) { return i == 0 ? 2 : 1; }
   __host__ __device__ static constexpr int c(int i, int a) {
     constexpr int t[5][3] = {{0, 0, 0}, {1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}};
     return t[i][a];
@@ -34,7 +51,8 @@ struct D2Q5 {
 };
 
 struct D3Q7 {
-  static constexpr int D = 3, Q = 7;
+  static constexpr int D = 3, Q = 7, kDen = 120;
+  __host__ __device__ static constexpr int wk(int i) { return i == 0 ? 6 : 19; }
   __host__ __device__ static constexpr int c(int i, int a) {
     constexpr int t[7][3] = {{0, 0, 0},  {1, 0, 0}, {-1, 0, 0}, {0, 1, 0},
                              {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
@@ -49,7 +67,10 @@ struct D3Q7 {
 };
 
 struct D3Q27 {
-  static constexpr int D = 3, Q = 27;
+  static constexpr int D = 3, Q = 27, kDen = 216;
+  __host__ __device__ static constexpr int wk(int i) {
+    return i == 0 ? 64 : (i < 7 ? 16 : (i < 19 ? 4 : 1));
+  }
   __host__ __device__ static constexpr int c(int i, int a) {
     constexpr int t[27][3] = {
         {0, 0, 0},   {1, 0, 0},  {-1, 0, 0},  {0, 1, 0},  {0, -1, 0}, {0, 0, 1},   {0, 0, -1},

@@ -5,6 +5,11 @@
 //              widened to float for the collision and rounded to nearest on store; this halves
 //              the bytes per cell update.
 // F64 : populations and every operation in double (the on-GPU FP64 comparison run).
+//
+// load/store move full population values f_i. load_dev/store_dev move deviations
+// d_i = f_i - W_i from the policy's offset W_i (the lattice weight in the compute precision):
+// the collision works on deviations, so for F32/F64 storage f_i = W_i + d_i is rounded once on
+// store, and for the 16-bit policies the stored value is the deviation itself.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -23,6 +28,8 @@ struct Pop<kF32> {
   using real = float;
   __device__ __forceinline__ static real load(const type* p, real) { return *p; }
   __device__ __forceinline__ static void store(type* p, real v, real) { *p = v; }
+  __device__ __forceinline__ static real load_dev(const type* p, real w) { return *p - w; }
+  __device__ __forceinline__ static void store_dev(type* p, real d, real w) { *p = w + d; }
 };
 
 template <>
@@ -34,6 +41,10 @@ struct Pop<kF16> {
   }
   __device__ __forceinline__ static void store(type* p, real v, real w) {
     *p = __float2half_rn(v - w);
+  }
+  __device__ __forceinline__ static real load_dev(const type* p, real) { return __half2float(*p); }
+  __device__ __forceinline__ static void store_dev(type* p, real d, real) {
+    *p = __float2half_rn(d);
   }
 };
 
@@ -47,6 +58,12 @@ struct Pop<kBF16> {
   __device__ __forceinline__ static void store(type* p, real v, real w) {
     *p = __float2bfloat16_rn(v - w);
   }
+  __device__ __forceinline__ static real load_dev(const type* p, real) {
+    return __bfloat162float(*p);
+  }
+  __device__ __forceinline__ static void store_dev(type* p, real d, real) {
+    *p = __float2bfloat16_rn(d);
+  }
 };
 
 template <>
@@ -55,6 +72,8 @@ struct Pop<kF64> {
   using real = double;
   __device__ __forceinline__ static real load(const type* p, real) { return *p; }
   __device__ __forceinline__ static void store(type* p, real v, real) { *p = v; }
+  __device__ __forceinline__ static real load_dev(const type* p, real w) { return *p - w; }
+  __device__ __forceinline__ static void store_dev(type* p, real d, real w) { *p = w + d; }
 };
 
 // Weight of slot i in the compute precision of the policy.
@@ -64,6 +83,20 @@ __host__ __device__ constexpr Real weight(int i) {
     return L::wd(i);
   else
     return L::w(i);
+}
+
+// Sum of the offsets minus one (the float weights sum to 1 + O(1e-8)); and the per-slot gap
+// between the exact weight wk/kDen and the offset W_i. Both are compile-time constants.
+template <class L, class Real>
+__host__ __device__ constexpr Real weight_defect() {
+  double s = 0;
+  for (int i = 0; i < L::Q; ++i) s += (double)weight<L, Real>(i);
+  return (Real)(s - 1.0);
+}
+
+template <class L, class Real>
+__host__ __device__ constexpr Real weight_gap(int i) {
+  return (Real)((double)L::wk(i) / (double)L::kDen - (double)weight<L, Real>(i));
 }
 
 }  // namespace lbm

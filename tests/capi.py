@@ -80,6 +80,12 @@ class CApiSim:
             check(_lib.lbm_download_tracer(self.h, t, _ptr(v)))
         self.iteration += n
 
+    def fluid_f64(self) -> tuple[np.ndarray, np.ndarray]:
+        rho = np.empty(self.counts, np.float64)
+        vel = np.empty(self.counts + [self.d], np.float64)
+        check(_lib.lbm_download_fluid_f64(self.h, _ptr(rho), _ptr(vel)))
+        return rho, vel
+
     def populations(self) -> np.ndarray:
         f = np.empty(self.counts + [self.q], np.float32)
         check(_lib.lbm_download_f(self.h, _ptr(f)))

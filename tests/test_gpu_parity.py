@@ -111,7 +111,7 @@ def _oracle_like(setup, backend):
     def omega_for(kind, tau):
         return OOmega.bgk(tau) if kind == "bgk" else OOmega.trt(tau)
 
-    first = omega_for(setup.collision, setup.tau)
+    first = OOmega.bgk(setup.tau) if setup.collision == "bgk" else OOmega.trt(setup.tau, setup.tau_neg)
     sim = OracleSimulation(setup.counts, first, backend=backend)
 
     def tracer_handle(s, name, om):
@@ -125,7 +125,7 @@ def _capi_like(setup, storage="f32"):
     from boltzmann_b200 import workloads
     from tests.capi import CApiSim
 
-    om = OOmega.bgk(setup.tau) if setup.collision == "bgk" else OOmega.trt(setup.tau)
+    om = OOmega.bgk(setup.tau) if setup.collision == "bgk" else OOmega.trt(setup.tau, setup.tau_neg)
     sim = CApiSim(setup.counts, om.kind, float(om.pos), float(om.neg), storage=storage)
 
     class Shim:  # the reference-API surface workloads.apply needs
@@ -254,3 +254,40 @@ def test_checkpoint_layout_round_trip_capi():
     b.iterate(4)
     np.testing.assert_array_equal(a.rho, b.rho)
     np.testing.assert_array_equal(a.populations(), b.populations())
+
+
+def test_f64_storage_matches_f64_oracle():
+    """The FP64 path against the FP64 oracle restatement (same algorithm in double)."""
+    from boltzmann_b200 import workloads
+
+    setup = workloads.cylinder_channel(128, 64, radius=4.0, re=100.0, buoyancy=1e-4)
+    gpu = _capi_like(setup, storage="f64")
+    gpu.iterate(100)
+    rho, vel = gpu.fluid_f64()
+    om = OOmega.trt(setup.tau, setup.tau_neg)
+    cpu = OracleSimulation(setup.counts, om, backend="port", precision="f64")
+
+    def tracer_handle(s, name, o):
+        return name, s.add_tracer(name, o).val
+
+    workloads.apply(cpu, setup, lambda k, t: OOmega.bgk(t), tracer_handle)
+    cpu.iterate(100)
+    assert rel_err(rho, cpu.rho) < 1e-12
+    assert rel_err(vel, cpu.vel) < 1e-10
+
+
+@pytest.mark.parametrize("storage,bound", [("f16", 1e-3), ("bf16", 2e-2), ("f32", 1e-5)])
+def test_storage_velocity_error_vs_f64(storage, bound):
+    """Velocity L2 error of each storage precision against an FP64 GPU run of the same
+    Taylor-Green vortex (D3Q27 BGK, 48^3, Re 400, 400 steps). North-star bound for FP16: 1e-3."""
+    from boltzmann_b200 import workloads
+
+    setup = workloads.taylor_green_3d(48, u0=0.05, re=400.0)
+    ref = _capi_like(setup, storage="f64")
+    ref.iterate(400)
+    _, vref = ref.fluid_f64()
+    run = _capi_like(setup, storage=storage)
+    run.iterate(400)
+    err = rel_err(run.vel, vref)
+    print(f"{storage}: velocity L2 error vs f64 = {err:.3e}")
+    assert err < bound
