@@ -5,7 +5,7 @@
 #include <atomic>
 #include <mutex>
 
-#include "aa_pipe.cuh"
+#include "aa_tma.cuh"
 #include "aa_step.cuh"
 #include "sim.h"
 
@@ -63,54 +63,51 @@ void step_geometry(const StepArgs<Real>& a, dim3& grid, dim3& block) {
   grid = dim3((a.nz + bx - 1) / bx, a.ny < 65535 ? a.ny : 65535, a.nx < 65535 ? a.nx : 65535);
 }
 
-// Pipeline depth: enough stages to cover DRAM latency within the shared memory of 2-3 CTAs per
-// SM (D2Q9 + D2Q5 F32: 64 KB per 256-thread CTA; D3Q27 F32: 89 KB; D3Q27 F64: 119 KB).
-template <class L, int K>
-constexpr int pipe_stages() {
-  return L::Q > 9 ? (sizeof(typename Pop<K>::type) == 8 ? 2 : 3) : 4;
+// Ring depth of the TMA kernel: as many stages as fit in ~96 KB per CTA (2-6), so that two or
+// three CTAs per SM keep several tiles of copies in flight.
+template <class L, int K, int NT, bool EVEN>
+constexpr int tma_stages() {
+  constexpr size_t b = TmaStage<L, K, NT, EVEN>::bytes;
+  constexpr int s = (int)((96 * 1024) / b);
+  return s < 2 ? 2 : (s > 6 ? 6 : s);
+}
+
+template <class L, bool TRT, int K, bool EVEN, int NT>
+cudaError_t launch_tma(const StepArgs<typename Pop<K>::real>& a, cudaStream_t stream) {
+  constexpr int S = tma_stages<L, K, NT, EVEN>();
+  constexpr size_t smem = tma_smem_bytes<L, K, NT, EVEN, S>();
+  auto kern = aa_tma_kernel<L, TRT, K, EVEN, NT, S>;
+  static std::once_flag once;
+  static cudaError_t setup_err = cudaSuccess;
+  static int per_sm = 1;
+  std::call_once(once, [&] {
+    setup_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (setup_err == cudaSuccess)
+      setup_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTmaTile, smem);
+    if (per_sm < 1) per_sm = 1;
+  });
+  if (setup_err != cudaSuccess) return setup_err;
+  int device = 0, sms = 148;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const long long tiles = (long long)a.nx * a.ny * (a.nz / kTmaTile);
+  long long grid = (long long)sms * per_sm;
+  if (grid > tiles) grid = tiles;
+  kern<<<(unsigned)grid, kTmaTile, smem, stream>>>(a);
+  return cudaGetLastError();
 }
 
 template <class L, bool TRT, int K, bool EVEN, int NT>
 cudaError_t launch_one(const StepArgs<typename Pop<K>::real>& a, cudaStream_t stream) {
-  if constexpr (sizeof(typename Pop<K>::type) == 2) {
-    dim3 grid, block;
-    step_geometry(a, grid, block);
-    aa_step_kernel<L, TRT, K, EVEN, NT><<<grid, block, 0, stream>>>(a);
-    return cudaGetLastError();
-  } else {
-    constexpr int S = pipe_stages<L, K>();
-    auto kern = aa_pipe_kernel<L, TRT, K, EVEN, NT, S>;
-    const int threads = a.nz >= 256 ? 256 : ((a.nz + 31) / 32) * 32;
-    const size_t smem = pipe_smem_bytes<L, K, NT, S>(threads);
-    static std::once_flag attr_once;
-    static cudaError_t attr_err = cudaSuccess;
-    std::call_once(attr_once, [&] {
-      attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)pipe_smem_bytes<L, K, NT, S>(256));
-    });
-    if (attr_err != cudaSuccess) return attr_err;
-    // Resident CTAs per SM for this block size, cached per instantiation.
-    static std::atomic<int> cached_threads{0}, cached_blocks{0};
-    int per_sm = cached_threads.load() == threads ? cached_blocks.load() : 0;
-    if (per_sm == 0) {
-      cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
-      if (e != cudaSuccess) return e;
-      if (per_sm < 1) per_sm = 1;
-      cached_blocks.store(per_sm);
-      cached_threads.store(threads);
-    }
-    int device = 0, sms = 148;
-    cudaGetDevice(&device);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    const int gx = (a.nz + threads - 1) / threads;
-    const long long rows = (long long)a.nx * a.ny;
-    long long gy = ((long long)sms * per_sm + gx - 1) / gx;
-    if (gy > rows) gy = rows;
-    if (gy > 65535) gy = 65535;
-    if (gy < 1) gy = 1;
-    kern<<<dim3(gx, (unsigned)gy, 1), threads, smem, stream>>>(a);
-    return cudaGetLastError();
+  // Rows that split into whole 256-cell tiles go through the TMA-staged kernel (fused tracers:
+  // none or one); everything else through the direct kernel.
+  if constexpr (NT >= 0) {
+    if (a.nz % kTmaTile == 0) return launch_tma<L, TRT, K, EVEN, NT>(a, stream);
   }
+  dim3 grid, block;
+  step_geometry(a, grid, block);
+  aa_step_kernel<L, TRT, K, EVEN, NT><<<grid, block, 0, stream>>>(a);
+  return cudaGetLastError();
 }
 
 template <class L, bool TRT, int K>

@@ -1,0 +1,265 @@
+// TMA-staged variant of the AA step: the main kernel for domains whose contiguous axis is a
+// multiple of 256 cells (kTmaTile).
+//
+// Work unit: a tile of T consecutive cells of one grid row (T threads, one cell each). A
+// persistent CTA walks its tiles with an S-stage ring in shared memory. For every tile, one
+// elected thread moves each operand row segment with a single bulk copy (cp.async.bulk, the TMA
+// engine, completion counted on the stage's mbarrier): per direction i the T populations the
+// tile needs -- on even steps slot i of the upstream row segment, which is shifted by -c_iz, so
+// the copy takes the 16-byte-aligned superset [z0 - H, z0 + T + H) with H = 16 / sizeof(T)
+// (pieces past the row ends come from the other end: the domain is periodic) -- plus the fused
+// tracer's populations, the coupled tracer value and the flag bytes.
+// Threads read their operands from shared memory (consecutive threads, consecutive words: no
+// bank conflicts), collide, and store straight to HBM with coalesced stores.
+//
+// In-flight data is bounded by shared memory, not by registers, and the copy engine issues one
+// instruction per row segment instead of one per element.
+//
+// Synchronisation per tile: wait on the stage's mbarrier (bounded: on timeout the kernel sets
+// bit 1 (value 2) of the status word and leaves), read the operands into registers, __syncthreads() (the stage is then
+// free), the elected thread refills the stage with tile k + S, then compute and store.
+// Every population slot is still read and written by exactly one thread per step, and no tile
+// writes what another tile of the same step reads, so stores need no ordering with the copies.
+#pragma once
+
+#include <cstdint>
+
+#include "aa_step.cuh"
+
+namespace lbm {
+
+constexpr int kTmaTile = 256;       // threads and cells per tile
+constexpr unsigned kSpinLimit = 1u << 22;  // mbarrier try_wait polls before giving up
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// Bounded wait for the phase with the given parity; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  const unsigned addr = smem_u32(bar);
+  for (unsigned i = 0; i < kSpinLimit; ++i) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// One bulk copy global -> shared, completing on `bar`. Addresses 16-byte aligned, size a
+// multiple of 16.
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+
+// Shared-memory layout of one stage, in elements of each operand's type.
+template <class L, int K, int NT, bool EVEN>
+struct TmaStage {
+  using T = typename Pop<K>::type;
+  using Real = typename Pop<K>::real;
+  using TL = typename TracerLattice<L::D>::type;
+  static constexpr int Q = L::Q;
+  static constexpr int NG = NT == 1 ? TL::Q : 0;
+  static constexpr int H = EVEN ? 16 / (int)sizeof(T) : 0;       // population halo
+  static constexpr int HG = EVEN ? 16 / (int)sizeof(Real) : 0;   // tracer halo
+  static constexpr int SEG = kTmaTile + 2 * H;                   // populations per direction
+  static constexpr int SEGG = kTmaTile + 2 * HG;
+  static constexpr size_t pop_bytes = (size_t)Q * SEG * sizeof(T);
+  static constexpr size_t trc_bytes = (size_t)NG * SEGG * sizeof(Real);
+  static constexpr size_t val_bytes = (size_t)kTmaTile * sizeof(Real);
+  static constexpr size_t flag_bytes = kTmaTile;
+  // offsets (bytes) inside a stage; every part 16-byte aligned
+  static constexpr size_t off_trc = pop_bytes;
+  static constexpr size_t off_val = off_trc + trc_bytes;
+  static constexpr size_t off_flag = off_val + val_bytes;
+  static constexpr size_t bytes = off_flag + flag_bytes;
+};
+
+template <class L, int K, int NT, bool EVEN, int S>
+__host__ __device__ constexpr size_t tma_smem_bytes() {
+  return (size_t)S * TmaStage<L, K, NT, EVEN>::bytes + 16 * S;  // + mbarriers
+}
+
+// Bulk-copies the row segment [z0 - h, z0 + T + h) of one operand row (elements of `es` bytes)
+// into dst, taking the parts left of 0 / right of nz from the other end of the row.
+__device__ __forceinline__ unsigned copy_row_segment(unsigned char* dst, const unsigned char* row,
+                                                     int z0, int h, int nz, int es,
+                                                     uint64_t* bar) {
+  const int lo = z0 - h, hi = z0 + kTmaTile + h;
+  unsigned bytes = 0;
+  if (lo < 0) {  // wrapped left halo: [nz + lo, nz)
+    bulk_copy(dst, row + (size_t)(nz + lo) * es, (unsigned)(-lo * es), bar);
+    bytes += (unsigned)(-lo * es);
+  }
+  const int a = lo < 0 ? 0 : lo, b = hi > nz ? nz : hi;
+  bulk_copy(dst + (size_t)(a - lo) * es, row + (size_t)a * es, (unsigned)((b - a) * es), bar);
+  bytes += (unsigned)((b - a) * es);
+  if (hi > nz) {  // wrapped right halo: [0, hi - nz)
+    bulk_copy(dst + (size_t)(nz - lo) * es, row, (unsigned)((hi - nz) * es), bar);
+    bytes += (unsigned)((hi - nz) * es);
+  }
+  return bytes;
+}
+
+template <class L, bool TRT, int K, bool EVEN, int NT, int S>
+__global__ void __launch_bounds__(kTmaTile)
+    aa_tma_kernel(const __grid_constant__ StepArgs<typename Pop<K>::real> a) {
+  using P = Pop<K>;
+  using Real = typename P::real;
+  using T = typename P::type;
+  using TL = typename TracerLattice<L::D>::type;
+  using St = TmaStage<L, K, NT, EVEN>;
+  constexpr int Q = L::Q;
+
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)S * St::bytes);
+  auto stage_ptr = [&](int s) { return smem + (size_t)s * St::bytes; };
+
+  const int tid = threadIdx.x;
+  const int tiles_per_row = a.nz / kTmaTile;
+  const long long ntiles = (long long)a.nx * a.ny * tiles_per_row;
+  // This CTA's tiles: blockIdx.x + j * gridDim.x, j = 0 .. count-1.
+  const int count =
+      (long long)blockIdx.x < ntiles ? (int)((ntiles - 1 - blockIdx.x) / gridDim.x + 1) : 0;
+
+  auto tile_origin = [&](int j, int& x, int& y, int& z0) {
+    const long long t = blockIdx.x + (long long)j * gridDim.x;
+    const long long row = t / tiles_per_row;
+    z0 = (int)(t - row * tiles_per_row) * kTmaTile;
+    x = (int)(row / a.ny);
+    y = (int)(row - (long long)x * a.ny);
+  };
+
+  // Elected thread: enqueue every operand of tile j into stage s.
+  auto produce = [&](int j, int s) {
+    if (j >= count) return;
+    int x, y, z0;
+    tile_origin(j, x, y, z0);
+    unsigned char* st = stage_ptr(s);
+    uint64_t* bar = bars + s;
+    const long long own_row = ((long long)x * a.ny + y) * a.nz;
+    const int xm = x == 0 ? a.nx - 1 : x - 1, xp = x == a.nx - 1 ? 0 : x + 1;
+    const int ym = y == 0 ? a.ny - 1 : y - 1, yp = y == a.ny - 1 ? 0 : y + 1;
+    // The expected byte count is fixed per stage; declare it before the copies.
+    unsigned expect = (unsigned)(Q * (kTmaTile + 2 * St::H) * sizeof(T) +
+                                 St::NG * (kTmaTile + 2 * St::HG) * sizeof(Real) + kTmaTile);
+    if (a.acc_mode == kAccBoussinesq) expect += kTmaTile * sizeof(Real);
+    mbar_expect_tx(bar, expect);
+    const T* f = static_cast<const T*>(a.f);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      const T* base;
+      if constexpr (EVEN) {
+        const int ux = upstream_coord(comp<L>(i, 0), xm, x, xp);
+        const int uy = upstream_coord(comp<L>(i, 1), ym, y, yp);
+        base = f + (long long)i * a.n + ((long long)ux * a.ny + uy) * a.nz;
+      } else {
+        base = f + (long long)opp(i) * a.n + own_row;
+      }
+      copy_row_segment(st + (size_t)i * St::SEG * sizeof(T),
+                       reinterpret_cast<const unsigned char*>(base), z0, St::H, a.nz, sizeof(T),
+                       bar);
+    }
+    if constexpr (NT == 1) {
+      const Real* g = a.tr[0].g;
+#pragma unroll
+      for (int i = 0; i < St::NG; ++i) {
+        const Real* base;
+        if constexpr (EVEN) {
+          const int ux = upstream_coord(comp<TL>(i, 0), xm, x, xp);
+          const int uy = upstream_coord(comp<TL>(i, 1), ym, y, yp);
+          base = g + (long long)i * a.n + ((long long)ux * a.ny + uy) * a.nz;
+        } else {
+          base = g + (long long)opp(i) * a.n + own_row;
+        }
+        copy_row_segment(st + St::off_trc + (size_t)i * St::SEGG * sizeof(Real),
+                         reinterpret_cast<const unsigned char*>(base), z0, St::HG, a.nz,
+                         sizeof(Real), bar);
+      }
+    }
+    if (a.acc_mode == kAccBoussinesq)
+      bulk_copy(st + St::off_val, a.coupled_val + own_row + z0, kTmaTile * sizeof(Real), bar);
+    bulk_copy(st + St::off_flag, a.flags + own_row + z0, kTmaTile, bar);
+  };
+
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) mbar_init(bars + s, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int s = 0; s < S; ++s) produce(s, s);
+
+  for (int j = 0; j < count; ++j) {
+    const int s = j % S;
+    const unsigned parity = (unsigned)((j / S) & 1);
+    const bool ok = mbar_wait(bars + s, parity);
+    if (!__syncthreads_and(ok)) {
+      // A copy never landed: report, give the copies still in flight a bounded chance to land
+      // (so none writes into shared memory after the CTA is gone), and stop this CTA.
+      if (tid == 0) {
+        atomicOr(a.status, 2);
+        for (int jj = j; jj < count && jj < j + S; ++jj) mbar_wait(bars + jj % S, (jj / S) & 1);
+      }
+      __syncthreads();
+      return;
+    }
+    int x, y, z0;
+    tile_origin(j, x, y, z0);
+    const unsigned char* st = stage_ptr(s);
+    Real fv[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      const T* seg = reinterpret_cast<const T*>(st + (size_t)i * St::SEG * sizeof(T));
+      const T v = EVEN ? seg[St::H + tid - comp<L>(i, 2)] : seg[tid];
+      fv[i] = P::load(&v, weight<L, Real>(i));
+    }
+    Real g[NT == 1 ? TL::Q : 1];
+    if constexpr (NT == 1) {
+#pragma unroll
+      for (int i = 0; i < St::NG; ++i) {
+        const Real* seg =
+            reinterpret_cast<const Real*>(st + St::off_trc + (size_t)i * St::SEGG * sizeof(Real));
+        g[i] = EVEN ? seg[St::HG + tid - comp<TL>(i, 2)] : seg[tid];
+      }
+    }
+    const Real cval = a.acc_mode == kAccBoussinesq
+                          ? reinterpret_cast<const Real*>(st + St::off_val)[tid]
+                          : Real(0);
+    const int flag = st[St::off_flag + tid];
+    __syncthreads();  // every thread has its operands: the stage can be refilled
+    if (tid == 0) {
+      fence_proxy_async();
+      produce(j + S, s);
+    }
+    const CellPos c = make_cellpos(a, x, y, z0 + tid, EVEN);
+    update_cell<L, TRT, K, EVEN, NT>(a, c, flag, fv, g, cval);
+  }
+}
+
+}  // namespace lbm

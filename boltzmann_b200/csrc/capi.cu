@@ -84,6 +84,17 @@ int download_reals(lbm_sim* s, float* dst, const void* src, int64_t count) {
   return LBM_OK;
 }
 
+// Reads the device status word after a synchronisation: bit 1 means a kernel gave up waiting for
+// its own asynchronous copies (it then stopped early and the state is not valid).
+int check_status(lbm_sim* s) {
+  int word = 0;
+  LBM_CUDA(cudaMemcpyAsync(&word, s->status, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  LBM_CUDA(cudaStreamSynchronize(s->stream));
+  if (word & 2)
+    return fail(LBM_ERR_CUDA, "an AA step gave up waiting for its staged copies (status bit 1)");
+  return LBM_OK;
+}
+
 void release(lbm_sim* s) {
   for (lbm_sim::Tracer& t : s->tracers) {
     cudaFree(t.g);
@@ -362,7 +373,7 @@ int lbm_download_fluid(lbm_sim* sim, float* rho, float* vel) {
     if (int rc = download_reals(sim, vel, sim->vel, sim->n * sim->dim)) return rc;
   }
   LBM_CUDA(cudaStreamSynchronize(sim->stream));
-  return LBM_OK;
+  return check_status(sim);
 }
 
 int lbm_download_tracer(lbm_sim* sim, int tracer, float* val) {
@@ -415,7 +426,7 @@ int lbm_nonfinite(lbm_sim* sim, int* out) {
 int lbm_synchronize(lbm_sim* sim) {
   if (int rc = activate(sim)) return rc;
   LBM_CUDA(cudaStreamSynchronize(sim->stream));
-  return LBM_OK;
+  return check_status(sim);
 }
 
 int lbm_stream(lbm_sim* sim, void** stream) {
