@@ -52,6 +52,7 @@ StepArgs<Real> make_step_args(const lbm_sim& s, bool write_moments) {
     a.tr[t].omega = s.tracers[t].omega;
   }
   a.write_moments = write_moments ? 1 : 0;
+  a.path = s.kernel_path;
   a.status = s.status;
   return a;
 }
@@ -83,7 +84,7 @@ cudaError_t launch_tma(const StepArgs<typename Pop<K>::real>& a, cudaStream_t st
   std::call_once(once, [&] {
     setup_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (setup_err == cudaSuccess)
-      setup_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTmaTile, smem);
+      setup_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTmaThreads, smem);
     if (per_sm < 1) per_sm = 1;
   });
   if (setup_err != cudaSuccess) return setup_err;
@@ -93,7 +94,7 @@ cudaError_t launch_tma(const StepArgs<typename Pop<K>::real>& a, cudaStream_t st
   const long long tiles = (long long)a.nx * a.ny * (a.nz / kTmaTile);
   long long grid = (long long)sms * per_sm;
   if (grid > tiles) grid = tiles;
-  kern<<<(unsigned)grid, kTmaTile, smem, stream>>>(a);
+  kern<<<(unsigned)grid, kTmaThreads, smem, stream>>>(a);
   return cudaGetLastError();
 }
 
@@ -101,8 +102,13 @@ template <class L, bool TRT, int K, bool EVEN, int NT>
 cudaError_t launch_one(const StepArgs<typename Pop<K>::real>& a, cudaStream_t stream) {
   // Rows that split into whole 256-cell tiles go through the TMA-staged kernel (fused tracers:
   // none or one); everything else through the direct kernel.
+  // Small domains (under ~8 tiles per SM; they sit in L2 anyway) stay on the direct kernel,
+  // whose launch has no ring to fill and drain.
   if constexpr (NT >= 0) {
-    if (a.nz % kTmaTile == 0) return launch_tma<L, TRT, K, EVEN, NT>(a, stream);
+    const long long tiles = (long long)a.nx * a.ny * (a.nz / kTmaTile);
+    const bool fits = a.nz % kTmaTile == 0;
+    const bool staged = a.path == 2 || (a.path == 0 && tiles >= 8LL * 148);
+    if (fits && staged) return launch_tma<L, TRT, K, EVEN, NT>(a, stream);
   }
   dim3 grid, block;
   step_geometry(a, grid, block);

@@ -59,6 +59,7 @@ struct StepArgs {
   int ntracers;
   TracerArgs<Real> tr[kMaxTracers];
   int write_moments;   // 1 on the last step of an iterate call
+  int path;            // kernel choice: 0 automatic, 1 direct, 2 TMA-staged (when the shape allows)
   int* status;         // bit 0 set when a non-finite density is produced
 };
 

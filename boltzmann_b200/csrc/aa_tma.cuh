@@ -2,8 +2,8 @@
 // multiple of 256 cells (kTmaTile).
 //
 // Work unit: a tile of T consecutive cells of one grid row (T threads, one cell each). A
-// persistent CTA walks its tiles with an S-stage ring in shared memory. For every tile, one
-// elected thread moves each operand row segment with a single bulk copy (cp.async.bulk, the TMA
+// persistent CTA walks its tiles with an S-stage ring in shared memory. For every tile, the
+// producer warp moves each operand row segment with a single bulk copy (cp.async.bulk, the TMA
 // engine, completion counted on the stage's mbarrier): per direction i the T populations the
 // tile needs -- on even steps slot i of the upstream row segment, which is shifted by -c_iz, so
 // the copy takes the 16-byte-aligned superset [z0 - H, z0 + T + H) with H = 16 / sizeof(T)
@@ -15,9 +15,11 @@
 // In-flight data is bounded by shared memory, not by registers, and the copy engine issues one
 // instruction per row segment instead of one per element.
 //
-// Synchronisation per tile: wait on the stage's mbarrier (bounded: on timeout the kernel sets
-// bit 1 (value 2) of the status word and leaves), read the operands into registers, __syncthreads() (the stage is then
-// free), the elected thread refills the stage with tile k + S, then compute and store.
+// Synchronisation: a producer warp fills stage s once every consumer warp has arrived on the
+// stage's `empty` barrier; consumers wait on its `full` barrier (expected bytes), read their
+// operands into registers, arrive on `empty`, then compute and store. There is no CTA-wide
+// barrier in the loop. Every wait is bounded: on timeout the kernel sets bit 1 (value 2) of the
+// status word and leaves.
 // Every population slot is still read and written by exactly one thread per step, and no tile
 // writes what another tile of the same step reads, so stores need no ordering with the copies.
 #pragma once
@@ -102,32 +104,34 @@ struct TmaStage {
 
 template <class L, int K, int NT, bool EVEN, int S>
 __host__ __device__ constexpr size_t tma_smem_bytes() {
-  return (size_t)S * TmaStage<L, K, NT, EVEN>::bytes + 16 * S;  // + mbarriers
+  return (size_t)S * TmaStage<L, K, NT, EVEN>::bytes + 16 * S;  // + full/empty mbarriers
 }
 
 // Bulk-copies the row segment [z0 - h, z0 + T + h) of one operand row (elements of `es` bytes)
 // into dst, taking the parts left of 0 / right of nz from the other end of the row.
-__device__ __forceinline__ unsigned copy_row_segment(unsigned char* dst, const unsigned char* row,
-                                                     int z0, int h, int nz, int es,
-                                                     uint64_t* bar) {
+__device__ __forceinline__ void copy_row_segment(unsigned char* dst, const unsigned char* row,
+                                                 int z0, int h, int nz, int es, uint64_t* bar) {
   const int lo = z0 - h, hi = z0 + kTmaTile + h;
-  unsigned bytes = 0;
-  if (lo < 0) {  // wrapped left halo: [nz + lo, nz)
+  if (lo < 0)  // wrapped left halo: [nz + lo, nz)
     bulk_copy(dst, row + (size_t)(nz + lo) * es, (unsigned)(-lo * es), bar);
-    bytes += (unsigned)(-lo * es);
-  }
   const int a = lo < 0 ? 0 : lo, b = hi > nz ? nz : hi;
   bulk_copy(dst + (size_t)(a - lo) * es, row + (size_t)a * es, (unsigned)((b - a) * es), bar);
-  bytes += (unsigned)((b - a) * es);
-  if (hi > nz) {  // wrapped right halo: [0, hi - nz)
+  if (hi > nz)  // wrapped right halo: [0, hi - nz)
     bulk_copy(dst + (size_t)(nz - lo) * es, row, (unsigned)((hi - nz) * es), bar);
-    bytes += (unsigned)((hi - nz) * es);
-  }
-  return bytes;
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
+constexpr int kConsumerWarps = kTmaTile / 32;
+constexpr int kTmaThreads = kTmaTile + 32;  // + one producer warp
+
+// Warp-specialised: warps 0..7 consume (one cell per thread), warp 8 produces. Stage s has a
+// `full` barrier (one arrival: the producer's expect_tx, plus the copies' bytes) and an `empty`
+// barrier (one arrival per consumer warp once it has its operands in registers).
 template <class L, bool TRT, int K, bool EVEN, int NT, int S>
-__global__ void __launch_bounds__(kTmaTile)
+__global__ void __launch_bounds__(kTmaThreads)
     aa_tma_kernel(const __grid_constant__ StepArgs<typename Pop<K>::real> a) {
   using P = Pop<K>;
   using Real = typename P::real;
@@ -135,12 +139,15 @@ __global__ void __launch_bounds__(kTmaTile)
   using TL = typename TracerLattice<L::D>::type;
   using St = TmaStage<L, K, NT, EVEN>;
   constexpr int Q = L::Q;
+  constexpr int NOPS = Q + St::NG + 2;  // copy jobs per tile: populations, tracer, value, flags
 
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)S * St::bytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)S * St::bytes);
+  uint64_t* empty = full + S;
   auto stage_ptr = [&](int s) { return smem + (size_t)s * St::bytes; };
 
   const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
   const int tiles_per_row = a.nz / kTmaTile;
   const long long ntiles = (long long)a.nx * a.ny * tiles_per_row;
   // This CTA's tiles: blockIdx.x + j * gridDim.x, j = 0 .. count-1.
@@ -155,79 +162,89 @@ __global__ void __launch_bounds__(kTmaTile)
     y = (int)(row - (long long)x * a.ny);
   };
 
-  // Elected thread: enqueue every operand of tile j into stage s.
-  auto produce = [&](int j, int s) {
-    if (j >= count) return;
-    int x, y, z0;
-    tile_origin(j, x, y, z0);
-    unsigned char* st = stage_ptr(s);
-    uint64_t* bar = bars + s;
-    const long long own_row = ((long long)x * a.ny + y) * a.nz;
-    const int xm = x == 0 ? a.nx - 1 : x - 1, xp = x == a.nx - 1 ? 0 : x + 1;
-    const int ym = y == 0 ? a.ny - 1 : y - 1, yp = y == a.ny - 1 ? 0 : y + 1;
-    // The expected byte count is fixed per stage; declare it before the copies.
-    unsigned expect = (unsigned)(Q * (kTmaTile + 2 * St::H) * sizeof(T) +
-                                 St::NG * (kTmaTile + 2 * St::HG) * sizeof(Real) + kTmaTile);
-    if (a.acc_mode == kAccBoussinesq) expect += kTmaTile * sizeof(Real);
-    mbar_expect_tx(bar, expect);
-    const T* f = static_cast<const T*>(a.f);
-#pragma unroll
-    for (int i = 0; i < Q; ++i) {
-      const T* base;
-      if constexpr (EVEN) {
-        const int ux = upstream_coord(comp<L>(i, 0), xm, x, xp);
-        const int uy = upstream_coord(comp<L>(i, 1), ym, y, yp);
-        base = f + (long long)i * a.n + ((long long)ux * a.ny + uy) * a.nz;
-      } else {
-        base = f + (long long)opp(i) * a.n + own_row;
-      }
-      copy_row_segment(st + (size_t)i * St::SEG * sizeof(T),
-                       reinterpret_cast<const unsigned char*>(base), z0, St::H, a.nz, sizeof(T),
-                       bar);
-    }
-    if constexpr (NT == 1) {
-      const Real* g = a.tr[0].g;
-#pragma unroll
-      for (int i = 0; i < St::NG; ++i) {
-        const Real* base;
-        if constexpr (EVEN) {
-          const int ux = upstream_coord(comp<TL>(i, 0), xm, x, xp);
-          const int uy = upstream_coord(comp<TL>(i, 1), ym, y, yp);
-          base = g + (long long)i * a.n + ((long long)ux * a.ny + uy) * a.nz;
-        } else {
-          base = g + (long long)opp(i) * a.n + own_row;
-        }
-        copy_row_segment(st + St::off_trc + (size_t)i * St::SEGG * sizeof(Real),
-                         reinterpret_cast<const unsigned char*>(base), z0, St::HG, a.nz,
-                         sizeof(Real), bar);
-      }
-    }
-    if (a.acc_mode == kAccBoussinesq)
-      bulk_copy(st + St::off_val, a.coupled_val + own_row + z0, kTmaTile * sizeof(Real), bar);
-    bulk_copy(st + St::off_flag, a.flags + own_row + z0, kTmaTile, bar);
-  };
-
   if (tid == 0) {
-    for (int s = 0; s < S; ++s) mbar_init(bars + s, 1);
+    for (int s = 0; s < S; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, kConsumerWarps);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
-  if (tid == 0)
-    for (int s = 0; s < S; ++s) produce(s, s);
 
+  if (warp == kConsumerWarps) {
+    // ---- producer warp: lane 0 declares the stage's bytes, then the lanes split the copies.
+    unsigned expect = (unsigned)(Q * St::SEG * sizeof(T) + St::NG * St::SEGG * sizeof(Real) +
+                                 kTmaTile);
+    if (a.acc_mode == kAccBoussinesq) expect += kTmaTile * sizeof(Real);
+    bool ok = true;
+    int produced = 0;
+    for (int j = 0; j < count && ok; ++j) {
+      const int s = j % S;
+      if (j >= S) ok = mbar_wait(empty + s, (unsigned)(((j / S) - 1) & 1));
+      if (!__all_sync(0xffffffffu, ok)) break;
+      int x, y, z0;
+      tile_origin(j, x, y, z0);
+      unsigned char* st = stage_ptr(s);
+      const long long own_row = ((long long)x * a.ny + y) * a.nz;
+      const int xm = x == 0 ? a.nx - 1 : x - 1, xp = x == a.nx - 1 ? 0 : x + 1;
+      const int ym = y == 0 ? a.ny - 1 : y - 1, yp = y == a.ny - 1 ? 0 : y + 1;
+      if (lane == 0) mbar_expect_tx(full + s, expect);
+      __syncwarp();
+      for (int op = lane; op < NOPS; op += 32) {
+        if (op < Q) {
+          const int i = op;
+          const T* base;
+          if constexpr (EVEN) {
+            const int ux = upstream_coord(comp<L>(i, 0), xm, x, xp);
+            const int uy = upstream_coord(comp<L>(i, 1), ym, y, yp);
+            base = static_cast<const T*>(a.f) + (long long)i * a.n +
+                   ((long long)ux * a.ny + uy) * a.nz;
+          } else {
+            base = static_cast<const T*>(a.f) + (long long)opp(i) * a.n + own_row;
+          }
+          copy_row_segment(st + (size_t)i * St::SEG * sizeof(T),
+                           reinterpret_cast<const unsigned char*>(base), z0, St::H, a.nz,
+                           sizeof(T), full + s);
+        } else if (op < Q + St::NG) {
+          if constexpr (NT == 1) {
+            const int i = op - Q;
+            const Real* base;
+            if constexpr (EVEN) {
+              const int ux = upstream_coord(comp<TL>(i, 0), xm, x, xp);
+              const int uy = upstream_coord(comp<TL>(i, 1), ym, y, yp);
+              base = a.tr[0].g + (long long)i * a.n + ((long long)ux * a.ny + uy) * a.nz;
+            } else {
+              base = a.tr[0].g + (long long)opp(i) * a.n + own_row;
+            }
+            copy_row_segment(st + St::off_trc + (size_t)i * St::SEGG * sizeof(Real),
+                             reinterpret_cast<const unsigned char*>(base), z0, St::HG, a.nz,
+                             sizeof(Real), full + s);
+          }
+        } else if (op == Q + St::NG) {
+          if (a.acc_mode == kAccBoussinesq)
+            bulk_copy(st + St::off_val, a.coupled_val + own_row + z0, kTmaTile * sizeof(Real),
+                      full + s);
+        } else {
+          bulk_copy(st + St::off_flag, a.flags + own_row + z0, kTmaTile, full + s);
+        }
+      }
+      produced = j + 1;
+    }
+    if (!ok && lane == 0) atomicOr(a.status, 2);
+    // Leave only once the copies of the last stages have landed (bounded), so that no copy
+    // writes into shared memory after the CTA is gone.
+    if (lane == 0)
+      for (int j = produced - S > 0 ? produced - S : 0; j < produced; ++j)
+        mbar_wait(full + j % S, (unsigned)((j / S) & 1));
+    return;
+  }
+
+  // ---- consumer warps: thread tid owns cell z0 + tid of every tile.
   for (int j = 0; j < count; ++j) {
     const int s = j % S;
-    const unsigned parity = (unsigned)((j / S) & 1);
-    const bool ok = mbar_wait(bars + s, parity);
-    if (!__syncthreads_and(ok)) {
-      // A copy never landed: report, give the copies still in flight a bounded chance to land
-      // (so none writes into shared memory after the CTA is gone), and stop this CTA.
-      if (tid == 0) {
-        atomicOr(a.status, 2);
-        for (int jj = j; jj < count && jj < j + S; ++jj) mbar_wait(bars + jj % S, (jj / S) & 1);
-      }
-      __syncthreads();
-      return;
+    if (!mbar_wait(full + s, (unsigned)((j / S) & 1))) {
+      atomicOr(a.status, 2);
+      return;  // the producer's own waits are bounded too
     }
     int x, y, z0;
     tile_origin(j, x, y, z0);
@@ -252,11 +269,8 @@ __global__ void __launch_bounds__(kTmaTile)
                           ? reinterpret_cast<const Real*>(st + St::off_val)[tid]
                           : Real(0);
     const int flag = st[St::off_flag + tid];
-    __syncthreads();  // every thread has its operands: the stage can be refilled
-    if (tid == 0) {
-      fence_proxy_async();
-      produce(j + S, s);
-    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(empty + s);  // this warp is done with stage s
     const CellPos c = make_cellpos(a, x, y, z0 + tid, EVEN);
     update_cell<L, TRT, K, EVEN, NT>(a, c, flag, fv, g, cval);
   }

@@ -423,6 +423,14 @@ int lbm_nonfinite(lbm_sim* sim, int* out) {
   return LBM_OK;
 }
 
+int lbm_set_kernel_path(lbm_sim* sim, int path) {
+  if (int rc = activate(sim)) return rc;
+  if (path < LBM_PATH_AUTO || path > LBM_PATH_STAGED)
+    return fail(LBM_ERR_ARGUMENT, "unknown kernel path");
+  sim->kernel_path = path;
+  return LBM_OK;
+}
+
 int lbm_synchronize(lbm_sim* sim) {
   if (int rc = activate(sim)) return rc;
   LBM_CUDA(cudaStreamSynchronize(sim->stream));

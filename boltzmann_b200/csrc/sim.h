@@ -26,6 +26,7 @@ struct lbm_sim {
   float om_pos = 0, om_neg = 0;
   int device = 0;
   cudaStream_t stream = nullptr;
+  int kernel_path = 0;  // LBM_PATH_AUTO / _DIRECT / _STAGED
 
   void* f = nullptr;    // [q][N] populations in the storage type
   void* rho = nullptr;  // [N], float (double for F64)

@@ -54,6 +54,12 @@ enum lbm_storage {
   LBM_STORAGE_F64 = 3   /* double populations and arithmetic (the FP64 comparison run) */
 };
 
+enum lbm_kernel_path {
+  LBM_PATH_AUTO = 0,   /* staged for large domains whose rows split into 256-cell tiles */
+  LBM_PATH_DIRECT = 1, /* one cell per thread, loads straight into registers */
+  LBM_PATH_STAGED = 2  /* TMA bulk copies into a shared-memory ring (rows of 256k cells only) */
+};
+
 /* Thread-local description of the last failure. */
 LBM_API const char* lbm_last_error(void);
 
@@ -137,6 +143,12 @@ LBM_API int lbm_conservation(lbm_sim* sim, double* out, int len);
  * since the last query, else 0; clears the flag. The device-side analogue of run_sim's NaN check
  * (python/boltzmann/simulation.py:241-242). Synchronous. */
 LBM_API int lbm_nonfinite(lbm_sim* sim, int* out);
+
+/* Chooses the AA kernel variant (enum lbm_kernel_path). A tuning and testing knob: results are
+ * identical up to floating-point rounding order; LBM_PATH_STAGED falls back to the direct kernel
+ * where the row length is not a multiple of 256 or more than one tracer is fused. No reference
+ * counterpart. */
+LBM_API int lbm_set_kernel_path(lbm_sim* sim, int path);
 
 /* Blocks until all work of the simulation is done. */
 LBM_API int lbm_synchronize(lbm_sim* sim);

@@ -29,7 +29,8 @@ def check(rc: int) -> None:
 class CApiSim:
     """One lbm_sim handle plus host arrays, with the reference's iterate semantics."""
 
-    def __init__(self, counts, kind: int, om_pos: float, om_neg: float = 0.0, q=None, storage="f32"):
+    def __init__(self, counts, kind: int, om_pos: float, om_neg: float = 0.0, q=None, storage="f32",
+                 path: str = "auto"):
         self.counts = [int(c) for c in counts]
         self.d = len(self.counts)
         self.q = q or {2: 9, 3: 27}[self.d]
@@ -39,6 +40,8 @@ class CApiSim:
             _lib.lbm_create(self.d, arr, self.q, kind, C.c_float(om_pos), C.c_float(om_neg),
                             STORAGE[storage], C.byref(self.h))
         )
+        if path != "auto":
+            self.set_kernel_path(path)
         self.flags = np.zeros(self.counts, np.int32)
         self.rho = np.ones(self.counts, np.float32)
         self.vel = np.zeros(self.counts + [self.d], np.float32)
@@ -108,6 +111,9 @@ class CApiSim:
         v = C.c_int()
         check(_lib.lbm_nonfinite(self.h, C.byref(v)))
         return bool(v.value)
+
+    def set_kernel_path(self, path: str) -> None:
+        check(_lib.lbm_set_kernel_path(self.h, {"auto": 0, "direct": 1, "staged": 2}[path]))
 
     def raw_iterate(self, n: int) -> int:
         return _lib.lbm_iterate(self.h, C.c_int64(n))

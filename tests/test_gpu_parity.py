@@ -34,11 +34,11 @@ def _omega_args(spec_omega):
     return o.kind, float(o.pos), float(o.neg)
 
 
-def _capi_from_spec(spec, inputs, storage="f32"):
+def _capi_from_spec(spec, inputs, storage="f32", path="auto"):
     from tests.capi import CApiSim
 
     kind, pos, neg = _omega_args(spec["omega"])
-    sim = CApiSim(spec["counts"], kind, pos, neg, storage=storage)
+    sim = CApiSim(spec["counts"], kind, pos, neg, storage=storage, path=path)
     sim.flags[...] = inputs["flags"]
     sim.rho[...] = inputs["rho"]
     sim.vel[...] = inputs["vel"]
@@ -329,13 +329,14 @@ def _oracle_from_spec(spec, inputs, precision="f32"):
     return sim
 
 
+@pytest.mark.parametrize("path", ["staged", "direct"])
 @pytest.mark.parametrize("name", sorted(TMA_CASES))
-def test_tma_path_vs_oracle(name):
+def test_tma_path_vs_oracle(name, path):
     from tests.golden.make_golden import seeded_inputs
 
     spec = TMA_CASES[name]
     inputs = seeded_inputs(spec, seed=11)
-    gpu, index = _capi_from_spec(spec, inputs)
+    gpu, index = _capi_from_spec(spec, inputs, path=path)
     cpu = _oracle_from_spec(spec, inputs)
     for n in spec["calls"]:
         gpu.iterate(n)
@@ -354,7 +355,7 @@ def test_tma_path_f64_vs_oracle_f64(name):
 
     spec = TMA_CASES[name]
     inputs = seeded_inputs(spec, seed=12)
-    gpu, index = _capi_from_spec(spec, inputs, storage="f64")
+    gpu, index = _capi_from_spec(spec, inputs, storage="f64", path="staged")
     cpu = _oracle_from_spec(spec, inputs, precision="f64")
     for n in spec["calls"]:
         gpu.iterate(n)
@@ -371,8 +372,8 @@ def test_tma_path_16bit_close_to_f32(storage):
 
     spec = TMA_CASES["d2q9_trt_tracer_coupling"]
     inputs = seeded_inputs(spec, seed=13)
-    a, _ = _capi_from_spec(spec, inputs, storage="f32")
-    b, _ = _capi_from_spec(spec, inputs, storage=storage)
+    a, _ = _capi_from_spec(spec, inputs, storage="f32", path="staged")
+    b, _ = _capi_from_spec(spec, inputs, storage=storage, path="staged")
     a.iterate(10)
     b.iterate(10)
     assert rel_err(b.rho, a.rho) < (1e-3 if storage == "f16" else 1e-2)
