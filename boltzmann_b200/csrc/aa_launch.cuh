@@ -64,13 +64,14 @@ void step_geometry(const StepArgs<Real>& a, dim3& grid, dim3& block) {
   grid = dim3((a.nz + bx - 1) / bx, a.ny < 65535 ? a.ny : 65535, a.nx < 65535 ? a.nx : 65535);
 }
 
-// Ring depth of the TMA kernel: as many stages as fit in ~96 KB per CTA (2-6), so that two or
-// three CTAs per SM keep several tiles of copies in flight.
+// Ring depth of the TMA kernel: as many stages as fit in ~50 KB per CTA (2-4), so that three or
+// four CTAs (24-32 consumer warps) share an SM and each keeps one or more tiles of copies in
+// flight while it computes another.
 template <class L, int K, int NT, bool EVEN>
 constexpr int tma_stages() {
   constexpr size_t b = TmaStage<L, K, NT, EVEN>::bytes;
-  constexpr int s = (int)((96 * 1024) / b);
-  return s < 2 ? 2 : (s > 6 ? 6 : s);
+  constexpr int s = (int)((50 * 1024) / b);
+  return s < 2 ? 2 : (s > 4 ? 4 : s);
 }
 
 template <class L, bool TRT, int K, bool EVEN, int NT>

@@ -80,19 +80,18 @@ __device__ __forceinline__ int upstream_coord(int cc, int minus1, int same, int 
   return cc > 0 ? minus1 : (cc < 0 ? plus1 : same);
 }
 
+// A cell and its periodic neighbourhood as 32-bit element offsets per axis:
+//   ox = {x-1, x, x+1} * ny * nz,  oy = {y-1, y, y+1} * nz,  oz = {z-1, z, z+1} (wrapped),
+// so the cell upstream of c_i is ox[.] + oy[.] + oz[.] (one three-input add) and every access is
+// a uniform per-direction base pointer plus a 32-bit offset. Cell counts stay below 2^32.
 struct CellPos {
-  long long cell;
-  int x, y, z;
-  int xm, xp, ym, yp, zm, zp;  // wrapped neighbour coordinates
-  int nx, ny, nz;
+  unsigned cell;
+  unsigned ox[3], oy[3], oz[3];
 
-  // Cell index of (x, y, z) - c_i, periodic.
   template <class L>
-  __device__ __forceinline__ long long upstream(int i) const {
-    const int ux = upstream_coord(comp<L>(i, 0), xm, x, xp);
-    const int uy = upstream_coord(comp<L>(i, 1), ym, y, yp);
-    const int uz = upstream_coord(comp<L>(i, 2), zm, z, zp);
-    return ((long long)ux * ny + uy) * nz + uz;
+  __device__ __forceinline__ unsigned upstream(int i) const {
+    // index 0: coordinate - 1 (component +1), 1: same, 2: coordinate + 1 (component -1)
+    return ox[1 - comp<L>(i, 0)] + oy[1 - comp<L>(i, 1)] + oz[1 - comp<L>(i, 2)];
   }
 };
 
@@ -105,7 +104,7 @@ __device__ __forceinline__ void aa_load(const typename P::type* __restrict__ f, 
 #pragma unroll
   for (int i = 0; i < L::Q; ++i) {
     const typename P::type* p =
-        EVEN ? f + (long long)i * n + c.upstream<L>(i) : f + (long long)opp(i) * n + c.cell;
+        EVEN ? (f + (size_t)i * n) + c.upstream<L>(i) : (f + (size_t)opp(i) * n) + c.cell;
     // Slot i (even) and slot opp(i) (odd) share the weight of direction i.
     if constexpr (DEV)
       v[i] = P::load_dev(p, weight<L, Real>(i));
@@ -121,7 +120,7 @@ __device__ __forceinline__ void aa_store(typename P::type* __restrict__ f, long 
   using Real = typename P::real;
 #pragma unroll
   for (int i = 0; i < L::Q; ++i) {
-    typename P::type* p = f + (long long)i * n + (EVEN ? c.upstream<L>(i) : c.cell);
+    typename P::type* p = (f + (size_t)i * n) + (EVEN ? c.upstream<L>(i) : c.cell);
     const Real val = EVEN ? v[opp(i)] : v[i];
     if constexpr (DEV)
       P::store_dev(p, val, weight<L, Real>(i));
@@ -207,20 +206,18 @@ template <class Real>
 __device__ __forceinline__ CellPos make_cellpos(const StepArgs<Real>& a, int x, int y, int z,
                                                 bool neighbours) {
   CellPos c;
-  c.nx = a.nx;
-  c.ny = a.ny;
-  c.nz = a.nz;
-  c.x = x;
-  c.y = y;
-  c.z = z;
-  c.cell = ((long long)x * a.ny + y) * a.nz + z;
+  const unsigned plane = (unsigned)a.ny * (unsigned)a.nz;
+  c.ox[1] = (unsigned)x * plane;
+  c.oy[1] = (unsigned)y * (unsigned)a.nz;
+  c.oz[1] = (unsigned)z;
+  c.cell = c.ox[1] + c.oy[1] + c.oz[1];
   if (neighbours) {
-    c.xm = x == 0 ? a.nx - 1 : x - 1;
-    c.xp = x == a.nx - 1 ? 0 : x + 1;
-    c.ym = y == 0 ? a.ny - 1 : y - 1;
-    c.yp = y == a.ny - 1 ? 0 : y + 1;
-    c.zm = z == 0 ? a.nz - 1 : z - 1;
-    c.zp = z == a.nz - 1 ? 0 : z + 1;
+    c.ox[0] = (unsigned)(x == 0 ? a.nx - 1 : x - 1) * plane;
+    c.ox[2] = (unsigned)(x == a.nx - 1 ? 0 : x + 1) * plane;
+    c.oy[0] = (unsigned)(y == 0 ? a.ny - 1 : y - 1) * (unsigned)a.nz;
+    c.oy[2] = (unsigned)(y == a.ny - 1 ? 0 : y + 1) * (unsigned)a.nz;
+    c.oz[0] = (unsigned)(z == 0 ? a.nz - 1 : z - 1);
+    c.oz[2] = (unsigned)(z == a.nz - 1 ? 0 : z + 1);
   }
   return c;
 }
@@ -286,7 +283,7 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
     r = a.rho[c.cell];
     dr = r - Real(1);
 #pragma unroll
-    for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] = a.vel[c.cell * L::D + ax - (3 - L::D)];
+    for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] = a.vel[(size_t)c.cell * L::D + ax - (3 - L::D)];
   }
   Real uu = 0;
 #pragma unroll
@@ -298,7 +295,7 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
   if (a.write_moments && !fixed) {
     a.rho[c.cell] = r;
 #pragma unroll
-    for (int ax = 3 - L::D; ax < 3; ++ax) a.vel[c.cell * L::D + ax - (3 - L::D)] = u[ax];
+    for (int ax = 3 - L::D; ax < 3; ++ax) a.vel[(size_t)c.cell * L::D + ax - (3 - L::D)] = u[ax];
     if (!isfinite(r)) atomicOr(a.status, 1);
   }
 

@@ -135,7 +135,8 @@ int lbm_create(int dim, const int64_t* counts, int q, int collision, float omega
       return fail(LBM_ERR_ARGUMENT, "cell counts must be positive");
     n *= counts[k];
   }
-  if (n > (int64_t)1 << 40) return fail(LBM_ERR_ARGUMENT, "domain too large");
+  // Kernels index cells with 32-bit offsets (populations are addressed per direction).
+  if (n >= ((int64_t)1 << 32)) return fail(LBM_ERR_ARGUMENT, "domain too large (2^32 cells)");
 
   lbm_sim* s = new (std::nothrow) lbm_sim();
   if (s == nullptr) return fail(LBM_ERR_ARGUMENT, "out of host memory");
