@@ -36,14 +36,17 @@ StepArgs<Real> make_step_args(const lbm_sim& s, bool write_moments) {
   if (!s.couplings.empty()) {
     const lbm_sim::Coupling& c = s.couplings.back();
     a.acc_mode = kAccBoussinesq;
-    for (int k = 0; k < s.dim; ++k) a.acc[off + k] = c.g[k];
+    // (g b) / om_pos in the reference (src/lib.cl:72 then 254); b (g / om_pos) here: the same
+    // shift up to one rounding of a term of the size of the buoyancy.
+    for (int k = 0; k < s.dim; ++k) a.force[off + k] = (Real)c.g[k] / (Real)s.om_pos;
     a.alpha = c.alpha;
     a.c0 = c.c0;
     a.coupled = c.tracer;
     a.coupled_val = static_cast<const Real*>(s.tracers[c.tracer].val);
   } else if (s.has_gravity) {
     a.acc_mode = kAccConstant;
-    for (int k = 0; k < s.dim; ++k) a.acc[off + k] = s.gravity[k];
+    // acc / om_pos, the division the reference makes per cell (src/lib.cl:254), made once.
+    for (int k = 0; k < s.dim; ++k) a.force[off + k] = (Real)s.gravity[k] / (Real)s.om_pos;
   }
   a.ntracers = (int)s.tracers.size();
   for (int t = 0; t < a.ntracers; ++t) {

@@ -52,7 +52,8 @@ struct StepArgs {
   long long n;         // cell count
   Real om_pos, om_neg; // BGK uses om_pos
   int acc_mode;        // 0: none, 1: constant acceleration acc[], 2: Boussinesq
-  Real acc[3];         // constant acceleration, or the Boussinesq gravity vector
+  Real force[3];       // velocity shift per unit buoyancy: acc / om_pos (constant acceleration,
+                       // the reference's per-cell division done once) or g / om_pos (Boussinesq)
   Real alpha, c0;      // Boussinesq coupling
   int coupled;         // index of the coupled tracer
   const Real* coupled_val;  // its val[] (read for the Boussinesq term)
@@ -148,8 +149,8 @@ __device__ __forceinline__ void aa_store(typename P::type* __restrict__ f, long 
 template <class L, bool TRT, bool DEV, class Real>
 __device__ __forceinline__ void collide(Real (&v)[L::Q], Real r, Real dr, const Real (&u)[3],
                                         Real uu, Real om_pos, Real om_neg) {
-  const Real ru = r / Real(L::kDen);
-  const Real unit = DEV ? dr / Real(L::kDen) : ru;  // the w_i (r or dr) term per unit weight
+  const Real ru = over_den<L>(r);
+  const Real unit = DEV ? over_den<L>(dr) : ru;  // the w_i (r or dr) term per unit weight
   const Real quad = Real(-1.5) * uu;
   {
     const Real k0 = Real(L::wk(0));
@@ -270,11 +271,11 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
   // Force as a velocity shift acc / omega (src/lib.cl:253-256; TRT: omega+, 682-685).
   if (a.acc_mode == kAccConstant) {
 #pragma unroll
-    for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] += a.acc[ax] / om_pos;
+    for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] += a.force[ax];
   } else if (a.acc_mode == kAccBoussinesq) {
-    const Real b = a.alpha * (cval - a.c0);
+    const Real b = a.alpha * (cval - a.c0);  // src/lib.cl:71
 #pragma unroll
-    for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] += (a.acc[ax] * b) / om_pos;
+    for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] += b * a.force[ax];
   }
   const bool fixed = (flag & 6) != 0;  // FIXED_FLUID_VELOCITY | FIXED_FLUID_DENSITY
   if (fixed) {                         // src/lib.cl:257-262

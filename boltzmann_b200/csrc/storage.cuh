@@ -99,4 +99,26 @@ __host__ __device__ constexpr Real weight_gap(int i) {
   return (Real)((double)L::wk(i) / (double)L::kDen - (double)weight<L, Real>(i));
 }
 
+// 1 / kDen as an unevaluated sum hi + lo of two values of the compute precision. x * (1/kDen)
+// evaluated as fma(x, hi, x * lo) is then the correctly rounded quotient up to a few units of
+// 2^-48 relative: unbiased like a division, at the cost of two instructions. (A single rounded
+// constant would scale every equilibrium weight by the same (1 + eps): a systematic mass drift.)
+template <class L, class Real>
+__host__ __device__ constexpr Real inv_den_hi() {
+  return (Real)(1.0 / (double)L::kDen);
+}
+
+template <class L, class Real>
+__host__ __device__ constexpr Real inv_den_lo() {
+  return (Real)(1.0 / (double)L::kDen - (double)inv_den_hi<L, Real>());
+}
+
+template <class L, class Real>
+__device__ __forceinline__ Real over_den(Real x) {
+  if constexpr (sizeof(Real) == 8)
+    return x / Real(L::kDen);
+  else
+    return fmaf(x, inv_den_hi<L, Real>(), x * inv_den_lo<L, Real>());
+}
+
 }  // namespace lbm
