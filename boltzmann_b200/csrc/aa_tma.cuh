@@ -172,10 +172,62 @@ __global__ void __launch_bounds__(kTmaThreads)
   __syncthreads();
 
   if (warp == kConsumerWarps) {
-    // ---- producer warp: lane 0 declares the stage's bytes, then the lanes split the copies.
+    // ---- producer warp. Each lane owns up to two copy jobs (job = lane, lane + 32), fixed for
+    // the whole kernel and described once here: source array, row shift (even steps read slot i
+    // of the row upstream of c_i), halo, element size, destination inside a stage.
+    struct Job {
+      const unsigned char* base;  // first element of the operand array (slot array for populations)
+      int cx, cy;                 // row shift: source row = (x - cx, y - cy)
+      int h, es;                  // halo (elements), element size (bytes)
+      unsigned dst;               // byte offset inside a stage
+      int kind;                   // 0 none, 1 row segment with halo, 2 own tile (no halo)
+    };
+    Job jobs[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int op = lane + 32 * k;
+      Job jb{nullptr, 0, 0, 0, 1, 0u, 0};
+      if (op < Q) {
+        const int slot = EVEN ? op : opp(op);
+        jb.base = reinterpret_cast<const unsigned char*>(static_cast<const T*>(a.f) +
+                                                         (size_t)slot * a.n);
+        jb.cx = EVEN ? comp<L>(op, 0) : 0;
+        jb.cy = EVEN ? comp<L>(op, 1) : 0;
+        jb.h = St::H;
+        jb.es = sizeof(T);
+        jb.dst = (unsigned)((size_t)op * St::SEG * sizeof(T));
+        jb.kind = 1;
+      } else if (op < Q + St::NG) {
+        if constexpr (NT == 1) {
+          const int i = op - Q;
+          const int slot = EVEN ? i : opp(i);
+          jb.base = reinterpret_cast<const unsigned char*>(a.tr[0].g + (size_t)slot * a.n);
+          jb.cx = EVEN ? comp<TL>(i, 0) : 0;
+          jb.cy = EVEN ? comp<TL>(i, 1) : 0;
+          jb.h = St::HG;
+          jb.es = sizeof(Real);
+          jb.dst = (unsigned)(St::off_trc + (size_t)i * St::SEGG * sizeof(Real));
+          jb.kind = 1;
+        }
+      } else if (op == Q + St::NG) {
+        if (a.acc_mode == kAccBoussinesq) {
+          jb.base = reinterpret_cast<const unsigned char*>(a.coupled_val);
+          jb.es = sizeof(Real);
+          jb.dst = (unsigned)St::off_val;
+          jb.kind = 2;
+        }
+      } else if (op == Q + St::NG + 1) {
+        jb.base = a.flags;
+        jb.es = 1;
+        jb.dst = (unsigned)St::off_flag;
+        jb.kind = 2;
+      }
+      jobs[k] = jb;
+    }
     unsigned expect = (unsigned)(Q * St::SEG * sizeof(T) + St::NG * St::SEGG * sizeof(Real) +
                                  kTmaTile);
     if (a.acc_mode == kAccBoussinesq) expect += kTmaTile * sizeof(Real);
+    const long long plane = (long long)a.ny * a.nz;
     bool ok = true;
     int produced = 0;
     for (int j = 0; j < count && ok; ++j) {
@@ -185,47 +237,22 @@ __global__ void __launch_bounds__(kTmaThreads)
       int x, y, z0;
       tile_origin(j, x, y, z0);
       unsigned char* st = stage_ptr(s);
-      const long long own_row = ((long long)x * a.ny + y) * a.nz;
       const int xm = x == 0 ? a.nx - 1 : x - 1, xp = x == a.nx - 1 ? 0 : x + 1;
       const int ym = y == 0 ? a.ny - 1 : y - 1, yp = y == a.ny - 1 ? 0 : y + 1;
       if (lane == 0) mbar_expect_tx(full + s, expect);
       __syncwarp();
-      for (int op = lane; op < NOPS; op += 32) {
-        if (op < Q) {
-          const int i = op;
-          const T* base;
-          if constexpr (EVEN) {
-            const int ux = upstream_coord(comp<L>(i, 0), xm, x, xp);
-            const int uy = upstream_coord(comp<L>(i, 1), ym, y, yp);
-            base = static_cast<const T*>(a.f) + (long long)i * a.n +
-                   ((long long)ux * a.ny + uy) * a.nz;
-          } else {
-            base = static_cast<const T*>(a.f) + (long long)opp(i) * a.n + own_row;
-          }
-          copy_row_segment(st + (size_t)i * St::SEG * sizeof(T),
-                           reinterpret_cast<const unsigned char*>(base), z0, St::H, a.nz,
-                           sizeof(T), full + s);
-        } else if (op < Q + St::NG) {
-          if constexpr (NT == 1) {
-            const int i = op - Q;
-            const Real* base;
-            if constexpr (EVEN) {
-              const int ux = upstream_coord(comp<TL>(i, 0), xm, x, xp);
-              const int uy = upstream_coord(comp<TL>(i, 1), ym, y, yp);
-              base = a.tr[0].g + (long long)i * a.n + ((long long)ux * a.ny + uy) * a.nz;
-            } else {
-              base = a.tr[0].g + (long long)opp(i) * a.n + own_row;
-            }
-            copy_row_segment(st + St::off_trc + (size_t)i * St::SEGG * sizeof(Real),
-                             reinterpret_cast<const unsigned char*>(base), z0, St::HG, a.nz,
-                             sizeof(Real), full + s);
-          }
-        } else if (op == Q + St::NG) {
-          if (a.acc_mode == kAccBoussinesq)
-            bulk_copy(st + St::off_val, a.coupled_val + own_row + z0, kTmaTile * sizeof(Real),
-                      full + s);
-        } else {
-          bulk_copy(st + St::off_flag, a.flags + own_row + z0, kTmaTile, full + s);
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const Job& jb = jobs[k];
+        if (jb.kind == 1) {
+          const int ux = jb.cx > 0 ? xm : (jb.cx < 0 ? xp : x);
+          const int uy = jb.cy > 0 ? ym : (jb.cy < 0 ? yp : y);
+          const unsigned char* row = jb.base + (size_t)(ux * plane + (long long)uy * a.nz) * jb.es;
+          copy_row_segment(st + jb.dst, row, z0, jb.h, a.nz, jb.es, full + s);
+        } else if (jb.kind == 2) {
+          const long long first = (long long)x * plane + (long long)y * a.nz + z0;
+          bulk_copy(st + jb.dst, jb.base + (size_t)first * jb.es, (unsigned)(kTmaTile * jb.es),
+                    full + s);
         }
       }
       produced = j + 1;
