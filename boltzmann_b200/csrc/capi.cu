@@ -110,6 +110,8 @@ void release(lbm_sim* s) {
 
 }  // namespace
 
+void lbm::set_last_error(const std::string& msg) { g_error = msg; }
+
 extern "C" {
 
 const char* lbm_last_error(void) { return g_error.c_str(); }

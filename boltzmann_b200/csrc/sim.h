@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <string>
 #include <vector>
 
 struct lbm_sim {
@@ -45,6 +46,9 @@ struct lbm_sim {
 };
 
 namespace lbm {
+
+// Sets the thread-local message returned by lbm_last_error().
+void set_last_error(const std::string& msg);
 
 // Bytes of one stored population for a storage kind.
 inline size_t pop_bytes(int storage) { return storage == 3 ? 8 : (storage == 0 ? 4 : 2); }

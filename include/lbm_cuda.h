@@ -156,6 +156,21 @@ LBM_API int lbm_synchronize(lbm_sim* sim);
 /* The simulation's cudaStream_t, for callers that time or order work around it. */
 LBM_API int lbm_stream(lbm_sim* sim, void** stream);
 
+/* The FP64 sums of lbm_conservation (sum f, then sum c_i f per axis) for a population array the
+ * caller owns, allocating no device memory: for callers that cannot allocate -- solvers embedded
+ * in another framework's memory arena or under an allocator that forbids extra cudaMalloc calls.
+ * No counterpart in the reference.
+ *   f      device pointer, layout [q][n] in the storage encoding of `storage` (the 16-bit kinds
+ *          hold f_i - w_i);
+ *   out    device pointer to 1 + dim doubles, all written;
+ *   stream cudaStream_t to run on (NULL: the default stream). Asynchronous.
+ * Scratch is a fixed 64 KiB per device inside this library, held until the process exits, so n is
+ * limited to 134,217,728 cells (LBM_ERR_ARGUMENT beyond). The first call on a device looks up that
+ * scratch's address; make it before any stream capture. All calls share the scratch: calls that
+ * may overlap on the GPU (unordered streams) race. */
+LBM_API int lbm_population_sums_noalloc(int dim, int q, int storage, const void* f, int64_t n,
+                                        double* out, void* stream);
+
 /* Page-locked host memory for host arrays (fast transfers); NULL on failure. */
 LBM_API void* lbm_host_alloc(size_t bytes);
 LBM_API void lbm_host_free(void* ptr);
