@@ -36,7 +36,7 @@ NVCC_FLAGS = [
     f"-I{INCLUDE}",
 ]
 
-CUDA_SOURCES = ["aa_d2q9.cu", "aa_d3q27.cu", "fields.cu", "capi.cu", "noalloc.cu"]
+CUDA_SOURCES = ["aa_d2q9.cu", "aa_d3q27.cu", "fields.cu", "capi.cu", "noalloc.cu", "ensemble.cu"]
 HEADERS = ["aa_step.cuh", "aa_tma.cuh", "aa_launch.cuh", "lattice.cuh", "storage.cuh", "sim.h"]
 
 

@@ -226,12 +226,16 @@ __device__ __forceinline__ CellPos make_cellpos(const StepArgs<Real>& a, int x, 
 // Everything after the loads for one cell: moments, forcing, fixed-cell override, collision,
 // AA store, end-of-call moments and the fused tracers. f holds the full population values of
 // the AA load, g the first tracer's (NT == 1), cval the coupled tracer's previous value.
+// om_pos / om_neg are the relaxation rates of the cell's domain (a.om_pos / a.om_neg for a single
+// simulation; per domain in an ensemble).
 template <class L, bool TRT, int K, bool EVEN, int NT>
 __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real>& a,
                                             const CellPos& c, int flag,
                                             typename Pop<K>::real (&f)[L::Q],
                                             typename Pop<K>::real (&g)[NT == 1 ? TracerLattice<L::D>::type::Q : 1],
-                                            typename Pop<K>::real cval) {
+                                            typename Pop<K>::real cval,
+                                            typename Pop<K>::real om_pos,
+                                            typename Pop<K>::real om_neg) {
   using P = Pop<K>;
   using Real = typename P::real;
   using T = typename P::type;
@@ -267,7 +271,6 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
 #pragma unroll
   for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] = u[ax] / r;
 
-  Real om_pos = a.om_pos, om_neg = a.om_neg;
   // Force as a velocity shift acc / omega (src/lib.cl:253-256; TRT: omega+, 682-685).
   if (a.acc_mode == kAccConstant) {
 #pragma unroll
@@ -339,7 +342,7 @@ __global__ void __launch_bounds__(256)
       if constexpr (NT == 1) aa_load<TL, TP, EVEN, false>(a.tr[0].g, a.n, c, g);
       Real cval = 0;
       if (a.acc_mode == kAccBoussinesq) cval = a.coupled_val[c.cell];
-      update_cell<L, TRT, K, EVEN, NT>(a, c, flag, f, g, cval);
+      update_cell<L, TRT, K, EVEN, NT>(a, c, flag, f, g, cval, a.om_pos, a.om_neg);
     }
   }
 }

@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(kTmaThreads)
     __syncwarp();
     if (lane == 0) mbar_arrive(empty + s);  // this warp is done with stage s
     const CellPos c = make_cellpos(a, x, y, z0 + tid, EVEN);
-    update_cell<L, TRT, K, EVEN, NT>(a, c, flag, fv, g, cval);
+    update_cell<L, TRT, K, EVEN, NT>(a, c, flag, fv, g, cval, a.om_pos, a.om_neg);
   }
 }
 

@@ -175,3 +175,67 @@ def apply(sim, setup: Setup, omega_for, tracer_handle=None) -> None:
         sim.set_gravity(np.asarray(setup.gravity, np.float32))
     for name, alpha, c0, g in setup.couplings:
         sim.add_boussinesq_coupling(handles[name], alpha, c0, np.asarray(g, np.float32))
+
+
+@dataclass
+class EnsembleSetup:
+    """Independent 2D domains for an ensemble run: per-domain counts and rates, plus the
+    concatenated host arrays (each domain in the reference's row-major order)."""
+
+    name: str
+    counts: list[tuple[int, int]]
+    tau: list[float]
+    flags: np.ndarray
+    rho: np.ndarray
+    vel: np.ndarray
+    params: dict = field(default_factory=dict)
+
+    @property
+    def cells(self) -> int:
+        return int(sum(a * b for a, b in self.counts))
+
+    def domain_slices(self) -> list[slice]:
+        out, start = [], 0
+        for a, b in self.counts:
+            out.append(slice(start, start + a * b))
+            start += a * b
+        return out
+
+
+def lid_driven_cavities(
+    count: int = 512,
+    lo: int = 64,
+    hi: int = 512,
+    u_lid: float = 0.05,
+    re_range: tuple[float, float] = (100.0, 5000.0),
+    seed: int = 0,
+) -> EnsembleSetup:
+    """``count`` square lid-driven cavities: side L ~ U{lo..hi}, Re ~ log-uniform on re_range,
+    tau = 1/2 + 3 u_lid L / Re (BGK). Walls on the left, right and bottom edges; the top row
+    (y = L-1, inner cells) is FIXED_FLUID with u = (u_lid, 0); rho = 1, fluid at rest."""
+    rng = np.random.default_rng(seed)
+    sides = rng.integers(lo, hi + 1, size=count)
+    res = np.exp(rng.uniform(np.log(re_range[0]), np.log(re_range[1]), size=count))
+    counts, taus, flags, rho, vel = [], [], [], [], []
+    for L, re in zip(sides.tolist(), res.tolist()):
+        fl = np.zeros((L, L), np.int32)
+        fl[0, :] = WALL
+        fl[-1, :] = WALL
+        fl[:, 0] = WALL
+        fl[1:-1, -1] = FIXED_FLUID
+        v = np.zeros((L, L, 2), np.float32)
+        v[1:-1, -1, 0] = u_lid
+        counts.append((L, L))
+        taus.append(0.5 + 3.0 * u_lid * L / re)
+        flags.append(fl.reshape(-1))
+        rho.append(np.ones(L * L, np.float32))
+        vel.append(v.reshape(-1, 2))
+    return EnsembleSetup(
+        "lid_driven_cavities",
+        counts,
+        taus,
+        np.concatenate(flags),
+        np.concatenate(rho),
+        np.concatenate(vel),
+        params={"u_lid": u_lid, "re": res.tolist(), "sides": sides.tolist()},
+    )

@@ -171,6 +171,39 @@ LBM_API int lbm_stream(lbm_sim* sim, void** stream);
 LBM_API int lbm_population_sums_noalloc(int dim, int q, int storage, const void* f, int64_t n,
                                         double* out, void* stream);
 
+/* ---- Batched ensembles of independent 2D D2Q9 domains (no reference counterpart: the reference
+ * runs one domain per Simulation). All domains advance together, one launch per step. ---- */
+typedef struct lbm_ensemble lbm_ensemble;
+
+enum lbm_ensemble_mode {
+  LBM_ENSEMBLE_PERSISTENT = 0, /* one persistent launch per step over the tile table */
+  LBM_ENSEMBLE_GRAPH = 1,      /* the same launches replayed from a captured CUDA graph */
+  LBM_ENSEMBLE_PER_DOMAIN = 2  /* one launch per domain per step (the unbatched baseline) */
+};
+
+/* counts: [ndomains][2] (nx, ny of each domain, the reference's 2D counts); omega_pos/omega_neg:
+ * per-domain BGK rate (or TRT rates; omega_neg may be NULL for BGK). Host arrays of an ensemble
+ * are the per-domain arrays concatenated in domain order (flags int32, rho, vel [.., 2]).
+ * Populations f32, f16 or bf16 (offsets). Each domain is periodic in itself. */
+LBM_API int lbm_ensemble_create(int ndomains, const int64_t* counts, int collision,
+                                const float* omega_pos, const float* omega_neg, int storage,
+                                lbm_ensemble** out);
+LBM_API int lbm_ensemble_destroy(lbm_ensemble* ens);
+LBM_API int lbm_ensemble_cells(lbm_ensemble* ens, int64_t* total);
+/* Tile shape: cells (threads) per tile, a multiple of 32 in [32, 512], and CTAs per SM of the
+ * persistent grid (0 = occupancy limit). Chosen by the autotuner (boltzmann_b200.autotune). */
+LBM_API int lbm_ensemble_set_shape(lbm_ensemble* ens, int tile_cells, int blocks_per_sm);
+LBM_API int lbm_ensemble_upload(lbm_ensemble* ens, const int32_t* flags, const float* rho,
+                                const float* vel);
+LBM_API int lbm_ensemble_equilibrate(lbm_ensemble* ens);
+/* iters even; mode: enum lbm_ensemble_mode. Asynchronous on the ensemble's stream. */
+LBM_API int lbm_ensemble_iterate(lbm_ensemble* ens, int64_t iters, int mode);
+LBM_API int lbm_ensemble_download(lbm_ensemble* ens, float* rho, float* vel);
+LBM_API int lbm_ensemble_upload_f(lbm_ensemble* ens, const float* f);
+LBM_API int lbm_ensemble_download_f(lbm_ensemble* ens, float* f);
+LBM_API int lbm_ensemble_stream(lbm_ensemble* ens, void** stream);
+LBM_API int lbm_ensemble_synchronize(lbm_ensemble* ens);
+
 /* Page-locked host memory for host arrays (fast transfers); NULL on failure. */
 LBM_API void* lbm_host_alloc(size_t bytes);
 LBM_API void lbm_host_free(void* ptr);

@@ -156,3 +156,29 @@ def test_checkpoint_velocity_sets_match_oracle():
         c, w, _ = velocity_set(d, q)
         np.testing.assert_array_equal(qs, c)
         np.testing.assert_array_equal(ws, w.astype(np.float32))
+
+
+def test_lid_driven_cavity_workload():
+    from boltzmann_b200 import workloads
+
+    s = workloads.lid_driven_cavities(count=16, lo=20, hi=40, seed=3)
+    assert len(s.counts) == 16 and s.cells == sum(a * b for a, b in s.counts)
+    for (a, b), sl, tau, re in zip(s.counts, s.domain_slices(), s.tau, s.params["re"]):
+        assert 20 <= a <= 40 and a == b
+        fl = s.flags[sl].reshape(a, b)
+        assert (fl[0] == 1).all() and (fl[-1] == 1).all() and (fl[:, 0] == 1).all()
+        assert (fl[1:-1, -1] == 6).all()
+        assert (s.vel[sl].reshape(a, b, 2)[1:-1, -1, 0] == np.float32(0.05)).all()
+        assert abs(tau - (0.5 + 3 * 0.05 * a / re)) < 1e-12
+        assert 100 <= re <= 5000
+
+
+def test_autotune_cache_key():
+    from boltzmann_b200 import autotune
+
+    class Fake:
+        counts = [(64, 64), (128, 128), (512, 512)]
+        n = 64 * 64 + 128 * 128 + 512 * 512
+        collision = 0
+
+    assert autotune.key(Fake(), "f32") == "D2Q9/bgk/f32/cells2^18-width2^7"
