@@ -1,7 +1,8 @@
 """Benchmark of the lattice-Boltzmann hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload cylinder_channel|kelvin_helmholtz|taylor_green_3d]
+                    [--workload cylinder_channel|kelvin_helmholtz|taylor_green_3d|
+                                cavity_ensemble|closure]
                     [--storage f32|f16|bf16|f64]
 
 One bench step is one AA step pair (two LBM time steps: the even and the odd kernel), the
@@ -50,7 +51,8 @@ def measured_peaks() -> tuple[dict, str]:
 def make_setup(workload: str):
     from boltzmann_b200 import workloads
 
-    if workload == "cylinder_channel":
+    if workload in ("cylinder_channel", "closure"):
+        # closure: the reference's way to that accuracy is the plain fine channel itself
         return workloads.cylinder_channel()
     if workload == "kelvin_helmholtz":
         return workloads.kelvin_helmholtz()
@@ -531,6 +533,120 @@ def run_ensemble(args) -> None:
         print(json.dumps(line), flush=True)
 
 
+def run_closure(args) -> None:
+    """The learned closure on the coarse 1024x512 analogue of the 4096x2048 cylinder channel:
+    data from seeded fine runs, training by the project's kernels, calibration on a training
+    seed, a posteriori judgement on a held-out seed. The value is the GPU-time ratio of the plain
+    fine run to the coarse+closure run over the same physical time, quoted at the closure's
+    accepted error (its mean relative velocity L2 error against the filtered fine run)."""
+    import torch
+
+    from boltzmann_b200 import closure as cl
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    cfg = cl.Config()
+    t0 = time.perf_counter()
+    data = cl.generate(cfg)
+    net, rep = cl.train(cfg, data)
+    S = data.rho.shape[0]
+    del data
+    cal = cl.calibrate(cfg, net, cl.Reference(cfg, cfg.calib_seed))
+    ref = cl.Reference(cfg, cfg.test_seed)
+    with ClockSampler(local) as clocks:
+        verdict = cl.judge(cfg, net, ref)
+    summary = verdict.summary()
+    t1 = time.perf_counter()
+    kind, _ = cl.run_closed_or_fine(cfg, verdict, net, ref)
+    e2e_s = time.perf_counter() - t1
+    pipeline_s = time.perf_counter() - t0
+
+    # Tensor-core roofline of the network's forward pass on a batch of coarse states.
+    nx, ny = cfg.coarse
+    B = 8
+    bufs = cl.Buffers(nx, ny, B, train=False)
+    bufs.x.zero_()
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(max(args.warmup, 3)):
+        cl.forward(net, bufs, stream)
+    reps = 20
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(reps):
+        cl.forward(net, bufs, stream)
+    ev1.record()
+    ev1.synchronize()
+    fwd_s = ev0.elapsed_time(ev1) / 1e3 / reps
+    flops = 21_312.0 * nx * ny * B  # 2 x (36 x 32 + 288 x 32 + 288) per cell
+    peaks, peak_kind = measured_peaks()
+    peak_tf = peaks.get("bf16_tflops", 1590.0)
+    achieved_tf = flops / fwd_s / 1e12
+
+    coarse_steps = cfg.horizons[-1]
+    line = {
+        "metric": "plain fine GPU time / coarse+closure GPU time, same physical time, at the "
+        "closure's accepted error",
+        "value": summary["time_ratio_fine_over_closure"],
+        "unit": "x",
+        "n_gpus": world,
+        "steps": coarse_steps,
+        "warmup": max(args.warmup, 3),
+        "ms_per_step": summary["closure_seconds"] * 1e3 / coarse_steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "bf16 network (fp32 accumulate), f32 stencil",
+        "data": "synthetic",
+        "config": {
+            "workload": f"closure: cylinder channel {cfg.coarse[0]}x{cfg.coarse[1]} (r "
+            f"{cfg.radius / cfg.factor:g}, Re {cfg.re:g}) vs {cfg.fine[0]}x{cfg.fine[1]}",
+            "network": "3x3 conv 4->32->32->1, GELU, BF16 weights, FP32 accumulation",
+            "target": "sqrt(k_sgs) of 4x4 box-filtered fine runs",
+            "every": cfg.every,
+            "train_seeds": list(cfg.train_seeds),
+            "test_seed": cfg.test_seed,
+            "snapshots": S,
+            "fine_steps_judged": verdict.fine_steps,
+            "l2": "stencil inputs larger than L2 at the fine size; no flush",
+        },
+        "closure": summary,
+        "calibration": cal,
+        "training": {"iters": rep.iters, "device_seconds": rep.seconds,
+                     "loss_first": rep.losses[0][1], "loss_last": rep.losses[-1][1]},
+        "roofline": {
+            "bound": "tensor",
+            "achieved": achieved_tf,
+            "peak": peak_tf,
+            "unit": "TFLOP/s",
+            "frac": achieved_tf / peak_tf,
+            "traffic": None,
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json bf16_tflops)",
+            "kernel": "closure forward (conv1 + conv32 mma.sync + conv3), batch 8 x 1024x512",
+            "flops_per_cell": 21_312,
+            "forward_ms": fwd_s * 1e3,
+        },
+        "cpu_baseline": None,
+        "e2e": {
+            "value": summary["fine_seconds"] / e2e_s,
+            "unit": "x",
+            "h2d_bytes_per_step": nx * ny * 16 / coarse_steps,
+            "d2h_bytes_per_step": nx * ny * 12 / coarse_steps,
+            "how": f"run_closed_or_fine ({kind}) from host arrays, host wall clock, against the "
+            "fine run's device time",
+        },
+        "gpu_launches": coarse_steps + 5 * (coarse_steps // cfg.every),
+        "clocks": clocks.summary(),
+        "pipeline_seconds": pipeline_s,
+    }
+    if not args.no_cpu_baseline:
+        cpu = cpu_reference_rate(cl.fine_setup(cfg, cfg.test_seed), args.cpu_seconds)
+        cpu["seconds_for_judged_fine_steps"] = (
+            cfg.fine[0] * cfg.fine[1] * verdict.fine_steps / (cpu["value"] * 1e6))
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -539,7 +655,7 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cylinder_channel",
                     choices=["cylinder_channel", "kelvin_helmholtz", "taylor_green_3d",
-                             "cavity_ensemble"])
+                             "cavity_ensemble", "closure"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f64"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -548,6 +664,8 @@ def main() -> None:
         run_reference(args)
     elif args.workload == "cavity_ensemble":
         run_ensemble(args)
+    elif args.workload == "closure":
+        run_closure(args)
     else:
         run_ours(args)
 

@@ -36,7 +36,7 @@ NVCC_FLAGS = [
     f"-I{INCLUDE}",
 ]
 
-CUDA_SOURCES = ["aa_d2q9.cu", "aa_d3q27.cu", "fields.cu", "capi.cu", "noalloc.cu", "ensemble.cu"]
+CUDA_SOURCES = ["aa_d2q9.cu", "aa_d3q27.cu", "fields.cu", "capi.cu", "noalloc.cu", "ensemble.cu", "closure.cu"]
 HEADERS = ["aa_step.cuh", "aa_tma.cuh", "aa_launch.cuh", "lattice.cuh", "storage.cuh", "sim.h"]
 
 
@@ -52,7 +52,7 @@ def _newer(target: Path, deps: list[Path]) -> bool:
 
 def build_cuda(force: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
-    headers = [CSRC / h for h in HEADERS] + [INCLUDE / "lbm_cuda.h"]
+    headers = [CSRC / h for h in HEADERS] + [INCLUDE / "lbm_cuda.h", INCLUDE / "lbm_closure.h"]
     jobs = []
     objs = []
     for src in CUDA_SOURCES:

@@ -56,6 +56,7 @@ StepArgs<Real> make_step_args(const lbm_sim& s, bool write_moments) {
   }
   a.write_moments = write_moments ? 1 : 0;
   a.path = s.kernel_path;
+  a.omega_field = s.omega_field;
   a.status = s.status;
   return a;
 }

@@ -61,6 +61,7 @@ struct StepArgs {
   TracerArgs<Real> tr[kMaxTracers];
   int write_moments;   // 1 on the last step of an iterate call
   int path;            // kernel choice: 0 automatic, 1 direct, 2 TMA-staged (when the shape allows)
+  const float* omega_field;  // per-cell om_pos (a learned closure's relaxation field), or null
   int* status;         // bit 0 set when a non-finite density is produced
 };
 
@@ -271,6 +272,8 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
 #pragma unroll
   for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] = u[ax] / r;
 
+  // A per-cell relaxation field replaces the domain's om_pos (the force shift keeps the domain's).
+  if (a.omega_field != nullptr) om_pos = (Real)__ldg(a.omega_field + c.cell);
   // Force as a velocity shift acc / omega (src/lib.cl:253-256; TRT: omega+, 682-685).
   if (a.acc_mode == kAccConstant) {
 #pragma unroll

@@ -434,6 +434,21 @@ int lbm_set_kernel_path(lbm_sim* sim, int path) {
   return LBM_OK;
 }
 
+int lbm_set_omega_field(lbm_sim* sim, const float* field) {
+  if (int rc = activate(sim)) return rc;
+  if (field != nullptr && sim->storage == LBM_STORAGE_F64)
+    return fail(LBM_ERR_UNSUPPORTED, "per-cell relaxation needs a float storage kind");
+  sim->omega_field = field;
+  return LBM_OK;
+}
+
+int lbm_fluid_device(lbm_sim* sim, void** rho, void** vel) {
+  if (int rc = activate(sim)) return rc;
+  if (rho) *rho = sim->rho;
+  if (vel) *vel = sim->vel;
+  return LBM_OK;
+}
+
 int lbm_synchronize(lbm_sim* sim) {
   if (int rc = activate(sim)) return rc;
   LBM_CUDA(cudaStreamSynchronize(sim->stream));

@@ -135,6 +135,15 @@ struct SimState {
   // with the GIL released.
   void iterate(int64_t iters) {
     if (iters % 2 != 0) throw Panic("iters must be even");
+    prepare();
+    check(lbm_iterate(h, iters));
+    read_back();
+    iteration += (uint64_t)iters;
+  }
+
+  // The device-side part of the first call (upload + equilibrate), late tracers, and the
+  // acceleration flag: everything iterate() does before stepping.
+  void prepare() {
     if (iteration == 0) {
       upload_all();
       check(lbm_equilibrate(h));
@@ -149,13 +158,15 @@ struct SimState {
       }
     }
     if (gravity || !couplings.empty()) acc_allocated = true;  // src/simulation.rs:288-295
-    check(lbm_iterate(h, iters));
+  }
+
+  // src/fields.rs:97-104, 177-183: device fields into the host mirrors.
+  void read_back() {
     check(lbm_download_fluid(h, rho.p, vel.p));
     for (auto& name : tracer_order) {
       TracerState& t = tracers.at(name);
       check(lbm_download_tracer(h, t.index, t.val.p));
     }
-    iteration += (uint64_t)iters;
   }
 };
 
@@ -486,12 +497,33 @@ PYBIND11_MODULE(boltzmann, m) {
            })
       .def("_iterate_device",
            [](Simulation& s, int64_t iters) {
-             // Steps only, without the read-back of iterate(): for device-side timing.
-             if (s.st->iteration == 0) throw Panic("call iterate() once before _iterate_device");
+             // Steps only, without the read-back of iterate() (device-side drivers and timing);
+             // _read_back() refreshes the host mirrors.
+             if (iters % 2 != 0) throw Panic("iters must be even");
              py::gil_scoped_release nogil;
              std::lock_guard<std::recursive_mutex> lock(s.st->mu);
+             s.st->prepare();
              check(lbm_iterate(s.st->h, iters));
              s.st->iteration += (uint64_t)iters;
+           })
+      .def("_read_back",
+           [](Simulation& s) {
+             py::gil_scoped_release nogil;
+             std::lock_guard<std::recursive_mutex> lock(s.st->mu);
+             s.st->read_back();
+           })
+      .def("_fluid_device",
+           [](const Simulation& s) {
+             // Device addresses of rho [N] and vel [N, D], current after each iterate call.
+             void *rho = nullptr, *vel = nullptr;
+             check(lbm_fluid_device(s.st->h, &rho, &vel));
+             return py::make_tuple(reinterpret_cast<uintptr_t>(rho), reinterpret_cast<uintptr_t>(vel));
+           })
+      .def("_set_omega_field",
+           [](Simulation& s, uintptr_t field) {
+             // Per-cell omega+ (device address of N floats, kept alive by the caller); 0 clears it.
+             std::lock_guard<std::recursive_mutex> lock(s.st->mu);
+             check(lbm_set_omega_field(s.st->h, reinterpret_cast<const float*>(field)));
            })
       .def("_synchronize", [](const Simulation& s) { check(lbm_synchronize(s.st->h)); })
       .def("_stream", [](const Simulation& s) {

@@ -28,6 +28,7 @@ struct lbm_sim {
   int device = 0;
   cudaStream_t stream = nullptr;
   int kernel_path = 0;  // LBM_PATH_AUTO / _DIRECT / _STAGED
+  const float* omega_field = nullptr;  // caller-owned per-cell om_pos, or null
 
   void* f = nullptr;    // [q][N] populations in the storage type
   void* rho = nullptr;  // [N], float (double for F64)

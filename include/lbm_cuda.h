@@ -150,6 +150,16 @@ LBM_API int lbm_nonfinite(lbm_sim* sim, int* out);
  * counterpart. */
 LBM_API int lbm_set_kernel_path(lbm_sim* sim, int path);
 
+/* Per-cell relaxation rate: `field` is a device array of N floats (omega+ of every cell) that
+ * the caller owns and keeps alive, written on the simulation's stream (a learned closure's output);
+ * NULL returns to the uniform rate. Fixed cells still relax with 1; the force shift keeps the
+ * uniform rate. Float storage kinds only. No reference counterpart. */
+LBM_API int lbm_set_omega_field(lbm_sim* sim, const float* field);
+
+/* Device pointers of rho [N] and vel [N, dim] (valid until lbm_destroy; written on the step that
+ * ends each lbm_iterate call), for device-side consumers on the simulation's stream. */
+LBM_API int lbm_fluid_device(lbm_sim* sim, void** rho, void** vel);
+
 /* Blocks until all work of the simulation is done. */
 LBM_API int lbm_synchronize(lbm_sim* sim);
 

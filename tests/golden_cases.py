@@ -11,7 +11,8 @@ GOLDEN = Path(__file__).resolve().parent / "golden"
 
 
 def names() -> list[str]:
-    return sorted(p.stem for p in GOLDEN.glob("*.npz"))
+    """The stencil fixtures (files with a case spec; postproc.npz holds other vectors)."""
+    return sorted(p.stem for p in GOLDEN.glob("*.npz") if "spec" in np.load(p).files)
 
 
 def load(name: str) -> tuple[dict, dict[str, np.ndarray], list[dict[str, np.ndarray]]]:
