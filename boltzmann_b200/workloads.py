@@ -82,7 +82,7 @@ def cylinder_channel(
 
     Bounce-back rows at y = 0 and y = ny-1, a bounce-back disc of ``radius`` at (nx/4, ny/2),
     fixed-velocity (and fixed-tracer) columns at x = 0 and x = nx-1 holding u = (u_in, 0).
-    nu = u_in * 2 radius / re, tau = 3 nu + 1/2 (TRT, magic 1/4). The D2Q5 tracer has
+    nu = u_in * 2 radius / re, tau+ = 3 nu + 1/2. The D2Q5 tracer has
     tau = 3 D + 1/2 and starts as a seeded random 0/1 band across the middle third of the
     channel height; it couples back with acc = g * alpha * C, alpha g = buoyancy * (0, -1).
     """
