@@ -6,9 +6,10 @@
 // producer warp moves each operand row segment with a single bulk copy (cp.async.bulk, the TMA
 // engine, completion counted on the stage's mbarrier): per direction i the T populations the
 // tile needs -- on even steps slot i of the upstream row segment, which is shifted by -c_iz, so
-// the copy takes the 16-byte-aligned superset [z0 - H, z0 + T + H) with H = 16 / sizeof(T)
-// (pieces past the row ends come from the other end: the domain is periodic) -- plus the fused
-// tracer's populations, the coupled tracer value and the flag bytes.
+// the copy takes a 16-byte-aligned superset with H = 16 / sizeof(T) extra elements on the side
+// the shift reaches (pieces past the row ends come from the other end: the domain is periodic;
+// when a row is a single tile the plain row is copied and the index wraps in shared memory) --
+// plus the fused tracer's populations, the coupled tracer value and the flag bytes.
 // Threads read their operands from shared memory (consecutive threads, consecutive words: no
 // bank conflicts), collide, and store straight to HBM with coalesced stores.
 //
@@ -107,11 +108,12 @@ __host__ __device__ constexpr size_t tma_smem_bytes() {
   return (size_t)S * TmaStage<L, K, NT, EVEN>::bytes + 16 * S;  // + full/empty mbarriers
 }
 
-// Bulk-copies the row segment [z0 - h, z0 + T + h) of one operand row (elements of `es` bytes)
+// Bulk-copies the row segment [z0 - hl, z0 + T + hr) of one operand row (elements of `es` bytes)
 // into dst, taking the parts left of 0 / right of nz from the other end of the row.
 __device__ __forceinline__ void copy_row_segment(unsigned char* dst, const unsigned char* row,
-                                                 int z0, int h, int nz, int es, uint64_t* bar) {
-  const int lo = z0 - h, hi = z0 + kTmaTile + h;
+                                                 int z0, int hl, int hr, int nz, int es,
+                                                 uint64_t* bar) {
+  const int lo = z0 - hl, hi = z0 + kTmaTile + hr;
   if (lo < 0)  // wrapped left halo: [nz + lo, nz)
     bulk_copy(dst, row + (size_t)(nz + lo) * es, (unsigned)(-lo * es), bar);
   const int a = lo < 0 ? 0 : lo, b = hi > nz ? nz : hi;
@@ -175,38 +177,48 @@ __global__ void __launch_bounds__(kTmaThreads)
     // ---- producer warp. Each lane owns up to two copy jobs (job = lane, lane + 32), fixed for
     // the whole kernel and described once here: source array, row shift (even steps read slot i
     // of the row upstream of c_i), halo, element size, destination inside a stage.
+    // A segment always lands so that its element z0 sits at index H of its slot in the stage.
+    // Even steps read z0 + t - c_iz: a direction with c_iz = +1 needs the left halo only, -1 the
+    // right one, 0 none. When a row is one tile (nz == T) the whole row is copied and consumers
+    // wrap the index instead, so no segment needs a halo or a wrapped piece.
     struct Job {
       const unsigned char* base;  // first element of the operand array (slot array for populations)
       int cx, cy;                 // row shift: source row = (x - cx, y - cy)
-      int h, es;                  // halo (elements), element size (bytes)
-      unsigned dst;               // byte offset inside a stage
+      int hl, hr, es;             // left / right halo (elements), element size (bytes)
+      unsigned dst;               // byte offset inside a stage of element z0 - hl
       int kind;                   // 0 none, 1 row segment with halo, 2 own tile (no halo)
     };
+    const bool whole_row = a.nz == kTmaTile;
     Job jobs[2];
+    unsigned lane_bytes = 0;
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       const int op = lane + 32 * k;
-      Job jb{nullptr, 0, 0, 0, 1, 0u, 0};
+      Job jb{nullptr, 0, 0, 0, 0, 1, 0u, 0};
       if (op < Q) {
         const int slot = EVEN ? op : opp(op);
+        const int cz = EVEN && !whole_row ? comp<L>(op, 2) : 0;
         jb.base = reinterpret_cast<const unsigned char*>(static_cast<const T*>(a.f) +
                                                          (size_t)slot * a.n);
         jb.cx = EVEN ? comp<L>(op, 0) : 0;
         jb.cy = EVEN ? comp<L>(op, 1) : 0;
-        jb.h = St::H;
+        jb.hl = cz > 0 ? St::H : 0;
+        jb.hr = cz < 0 ? St::H : 0;
         jb.es = sizeof(T);
-        jb.dst = (unsigned)((size_t)op * St::SEG * sizeof(T));
+        jb.dst = (unsigned)(((size_t)op * St::SEG + St::H - jb.hl) * sizeof(T));
         jb.kind = 1;
       } else if (op < Q + St::NG) {
         if constexpr (NT == 1) {
           const int i = op - Q;
           const int slot = EVEN ? i : opp(i);
+          const int cz = EVEN && !whole_row ? comp<TL>(i, 2) : 0;
           jb.base = reinterpret_cast<const unsigned char*>(a.tr[0].g + (size_t)slot * a.n);
           jb.cx = EVEN ? comp<TL>(i, 0) : 0;
           jb.cy = EVEN ? comp<TL>(i, 1) : 0;
-          jb.h = St::HG;
+          jb.hl = cz > 0 ? St::HG : 0;
+          jb.hr = cz < 0 ? St::HG : 0;
           jb.es = sizeof(Real);
-          jb.dst = (unsigned)(St::off_trc + (size_t)i * St::SEGG * sizeof(Real));
+          jb.dst = (unsigned)(St::off_trc + ((size_t)i * St::SEGG + St::HG - jb.hl) * sizeof(Real));
           jb.kind = 1;
         }
       } else if (op == Q + St::NG) {
@@ -223,10 +235,9 @@ __global__ void __launch_bounds__(kTmaThreads)
         jb.kind = 2;
       }
       jobs[k] = jb;
+      if (jb.kind != 0) lane_bytes += (unsigned)((kTmaTile + jb.hl + jb.hr) * jb.es);
     }
-    unsigned expect = (unsigned)(Q * St::SEG * sizeof(T) + St::NG * St::SEGG * sizeof(Real) +
-                                 kTmaTile);
-    if (a.acc_mode == kAccBoussinesq) expect += kTmaTile * sizeof(Real);
+    const unsigned expect = __reduce_add_sync(0xffffffffu, lane_bytes);
     const long long plane = (long long)a.ny * a.nz;
     bool ok = true;
     int produced = 0;
@@ -248,7 +259,7 @@ __global__ void __launch_bounds__(kTmaThreads)
           const int ux = jb.cx > 0 ? xm : (jb.cx < 0 ? xp : x);
           const int uy = jb.cy > 0 ? ym : (jb.cy < 0 ? yp : y);
           const unsigned char* row = jb.base + (size_t)(ux * plane + (long long)uy * a.nz) * jb.es;
-          copy_row_segment(st + jb.dst, row, z0, jb.h, a.nz, jb.es, full + s);
+          copy_row_segment(st + jb.dst, row, z0, jb.hl, jb.hr, a.nz, jb.es, full + s);
         } else if (jb.kind == 2) {
           const long long first = (long long)x * plane + (long long)y * a.nz + z0;
           bulk_copy(st + jb.dst, jb.base + (size_t)first * jb.es, (unsigned)(kTmaTile * jb.es),
@@ -267,6 +278,7 @@ __global__ void __launch_bounds__(kTmaThreads)
   }
 
   // ---- consumer warps: thread tid owns cell z0 + tid of every tile.
+  const bool whole_row = a.nz == kTmaTile;
   for (int j = 0; j < count; ++j) {
     const int s = j % S;
     if (!mbar_wait(full + s, (unsigned)((j / S) & 1))) {
@@ -280,7 +292,8 @@ __global__ void __launch_bounds__(kTmaThreads)
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
       const T* seg = reinterpret_cast<const T*>(st + (size_t)i * St::SEG * sizeof(T));
-      const T v = EVEN ? seg[St::H + tid - comp<L>(i, 2)] : seg[tid];
+      const int zi = whole_row ? (tid - comp<L>(i, 2)) & (kTmaTile - 1) : tid - comp<L>(i, 2);
+      const T v = EVEN ? seg[St::H + zi] : seg[tid];
       fv[i] = P::load(&v, weight<L, Real>(i));
     }
     Real g[NT == 1 ? TL::Q : 1];
@@ -289,7 +302,8 @@ __global__ void __launch_bounds__(kTmaThreads)
       for (int i = 0; i < St::NG; ++i) {
         const Real* seg =
             reinterpret_cast<const Real*>(st + St::off_trc + (size_t)i * St::SEGG * sizeof(Real));
-        g[i] = EVEN ? seg[St::HG + tid - comp<TL>(i, 2)] : seg[tid];
+        const int zi = whole_row ? (tid - comp<TL>(i, 2)) & (kTmaTile - 1) : tid - comp<TL>(i, 2);
+        g[i] = EVEN ? seg[St::HG + zi] : seg[tid];
       }
     }
     const Real cval = a.acc_mode == kAccBoussinesq
