@@ -294,7 +294,10 @@ __global__ void __launch_bounds__(kTmaThreads)
       const T* seg = reinterpret_cast<const T*>(st + (size_t)i * St::SEG * sizeof(T));
       const int zi = whole_row ? (tid - comp<L>(i, 2)) & (kTmaTile - 1) : tid - comp<L>(i, 2);
       const T v = EVEN ? seg[St::H + zi] : seg[tid];
-      fv[i] = P::load(&v, weight<L, Real>(i));
+      if constexpr (dev_in<K>())
+        fv[i] = P::load_dev(&v, weight<L, Real>(i));
+      else
+        fv[i] = P::load(&v, weight<L, Real>(i));
     }
     Real g[NT == 1 ? TL::Q : 1];
     if constexpr (NT == 1) {

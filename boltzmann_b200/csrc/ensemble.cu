@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(512)
     }
     const int flag = a.flags[c.cell];
     Real f[D2Q9::Q];
-    aa_load<D2Q9, P, EVEN, false>(static_cast<const T*>(a.f), a.n, c, f);
+    aa_load<D2Q9, P, EVEN, lbm::dev_in<K>()>(static_cast<const T*>(a.f), a.n, c, f);
     Real g[1];
     update_cell<D2Q9, TRT, K, EVEN, 0>(a, c, flag, f, g, Real(0), (Real)dom.om_pos,
                                        (Real)dom.om_neg);

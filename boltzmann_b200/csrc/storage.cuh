@@ -76,6 +76,14 @@ struct Pop<kF64> {
   __device__ __forceinline__ static void store_dev(type* p, real d, real w) { *p = w + d; }
 };
 
+// 16-bit kinds store deviations f_i - W_i; the update takes them as loaded, without forming the
+// full values (their rounding, ~1e-3 relative, dwarfs any FP32 ordering effect). FP32 and FP64
+// load full values, whose momentum sum is the reference's.
+template <int K>
+__host__ __device__ constexpr bool dev_in() {
+  return K == kF16 || K == kBF16;
+}
+
 // Weight of slot i in the compute precision of the policy.
 template <class L, class Real>
 __host__ __device__ constexpr Real weight(int i) {
