@@ -156,12 +156,31 @@ __global__ void __launch_bounds__(kTmaThreads)
   const int count =
       (long long)blockIdx.x < ntiles ? (int)((ntiles - 1 - blockIdx.x) / gridDim.x + 1) : 0;
 
-  auto tile_origin = [&](int j, int& x, int& y, int& z0) {
-    const long long t = blockIdx.x + (long long)j * gridDim.x;
-    const long long row = t / tiles_per_row;
-    z0 = (int)(t - row * tiles_per_row) * kTmaTile;
-    x = (int)(row / a.ny);
-    y = (int)(row - (long long)x * a.ny);
+  // This CTA's tiles in order, t = blockIdx.x + j * gridDim.x, as (x, y, tile within the row),
+  // advanced by a fixed stride with carries: no division per tile (every thread walks the
+  // tiles, so a division here would cost every cell).
+  struct TileWalker {
+    int x, y, zt, dx, dy, dz, ny, tpr;
+    __device__ void init(long long t0, long long stride, int ny_, int tpr_) {
+      ny = ny_;
+      tpr = tpr_;
+      const long long row = t0 / tpr, drow = stride / tpr;
+      zt = (int)(t0 - row * tpr);
+      dz = (int)(stride - drow * tpr);
+      y = (int)(row % ny);
+      x = (int)(row / ny);
+      dy = (int)(drow % ny);
+      dx = (int)(drow / ny);
+    }
+    __device__ void next() {
+      zt += dz;
+      const int carry = zt >= tpr ? 1 : 0;
+      zt -= carry * tpr;
+      y += dy + carry;
+      const int cy = y >= ny ? 1 : 0;
+      y -= cy * ny;
+      x += dx + cy;
+    }
   };
 
   if (tid == 0) {
@@ -241,12 +260,13 @@ __global__ void __launch_bounds__(kTmaThreads)
     const long long plane = (long long)a.ny * a.nz;
     bool ok = true;
     int produced = 0;
-    for (int j = 0; j < count && ok; ++j) {
+    TileWalker tw;
+    tw.init(blockIdx.x, gridDim.x, a.ny, tiles_per_row);
+    for (int j = 0; j < count && ok; ++j, tw.next()) {
       const int s = j % S;
       if (j >= S) ok = mbar_wait(empty + s, (unsigned)(((j / S) - 1) & 1));
       if (!__all_sync(0xffffffffu, ok)) break;
-      int x, y, z0;
-      tile_origin(j, x, y, z0);
+      const int x = tw.x, y = tw.y, z0 = tw.zt * kTmaTile;
       unsigned char* st = stage_ptr(s);
       const int xm = x == 0 ? a.nx - 1 : x - 1, xp = x == a.nx - 1 ? 0 : x + 1;
       const int ym = y == 0 ? a.ny - 1 : y - 1, yp = y == a.ny - 1 ? 0 : y + 1;
@@ -279,14 +299,15 @@ __global__ void __launch_bounds__(kTmaThreads)
 
   // ---- consumer warps: thread tid owns cell z0 + tid of every tile.
   const bool whole_row = a.nz == kTmaTile;
-  for (int j = 0; j < count; ++j) {
+  TileWalker tw;
+  tw.init(blockIdx.x, gridDim.x, a.ny, tiles_per_row);
+  for (int j = 0; j < count; ++j, tw.next()) {
     const int s = j % S;
     if (!mbar_wait(full + s, (unsigned)((j / S) & 1))) {
       atomicOr(a.status, 2);
       return;  // the producer's own waits are bounded too
     }
-    int x, y, z0;
-    tile_origin(j, x, y, z0);
+    const int x = tw.x, y = tw.y, z0 = tw.zt * kTmaTile;
     const unsigned char* st = stage_ptr(s);
     Real fv[Q];
 #pragma unroll
