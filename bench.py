@@ -2,7 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload cylinder_channel|kelvin_helmholtz|taylor_green_3d|
-                                cavity_ensemble|closure]
+                                cavity_ensemble|closure|closure_forward]
                     [--storage f32|f16|bf16|f64]
 
 One bench step is one AA step pair (two LBM time steps: the even and the odd kernel), the
@@ -310,6 +310,11 @@ def run_ours(args) -> None:
     tag = {"cylinder_channel": "d2q9_trt_tracer", "kelvin_helmholtz": "d2q9_bgk",
            "taylor_green_3d": "d3q27_bgk"}[args.workload] + f"_{args.storage}"
     traffic_pc = profiled_traffic(tag)
+    # The library's own choice (csrc/aa_launch.cuh launch_one): rows of whole 256-cell tiles and
+    # at least 8 tiles per SM go through the TMA-staged kernel, everything else the direct one.
+    nz = setup.counts[-1]
+    tiles = setup.cells // 256 if nz % 256 == 0 else 0
+    kernel = "aa_tma_kernel" if nz % 256 == 0 and tiles >= 8 * 148 else "aa_step_kernel"
 
     # End to end through the public API with host buffers: a fresh Simulation from host arrays;
     # one iterate(2K) call uploads flags/rho/vel/C, equilibrates, steps and reads rho/vel/C back.
@@ -357,7 +362,7 @@ def run_ours(args) -> None:
                 "traffic": None if traffic_pc is None else traffic_pc * setup.cells,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "algorithmic_bytes_per_cell_update": bpc,
-                "kernel": f"aa_step_kernel ({tag})",
+                "kernel": f"{kernel} ({tag})",
                 "frac_of_nominal_8tbs": achieved / 8000.0,
             },
             "cpu_baseline": cpu,
@@ -647,6 +652,68 @@ def run_closure(args) -> None:
         print(json.dumps(line), flush=True)
 
 
+def run_closure_forward(args) -> None:
+    """Kernel-level line for the closure network: K forward passes over a batch of 8 coarse
+    1024x512 states (random weights and inputs), device-timed, against the BF16 tensor peak."""
+    import torch
+
+    from boltzmann_b200 import closure as cl
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    nx, ny, B = 1024, 512, 8
+    rng = np.random.default_rng(0)
+    params = rng.uniform(-0.06, 0.06, cl.NPARAMS).astype(np.float32)
+    net = cl.Net(params, np.array([0, 0, 0, 0, 1, 1, 1, 1], np.float32))
+    bufs = cl.Buffers(nx, ny, B, train=False)
+    x = torch.tensor(rng.normal(size=nx * ny * B * 4).astype(np.float32), device="cuda")
+    bufs.x.copy_(x.to(torch.bfloat16).view(torch.int16))
+    stream = torch.cuda.current_stream().cuda_stream
+    K, W = args.steps, max(args.warmup, 3)
+    for _ in range(W):
+        cl.forward(net, bufs, stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        e0.record()
+        for _ in range(K):
+            cl.forward(net, bufs, stream)
+        e1.record()
+        e1.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    flops = 21_312.0 * nx * ny * B
+    peaks, peak_kind = measured_peaks()
+    peak = peaks.get("bf16_tflops", 1590.0)
+    achieved = flops / (ms * 1e-3) / 1e12
+    line = {
+        "metric": "closure forward TFLOP/s",
+        "value": achieved * world,
+        "unit": "TFLOP/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "bf16 (fp32 accumulate)",
+        "data": "synthetic",
+        "config": {"workload": "closure network forward, batch 8 x 1024x512, 3x3 conv "
+                               "4->32->32->1", "flops_per_cell": 21_312,
+                   "l2": "activations 2 x 268 MB per pass exceed L2; no flush"},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json bf16_tflops)",
+                     "kernel": "conv1_fwd + conv32_kernel (mma.sync) + conv3_fwd"},
+        "cpu_baseline": None,
+        "e2e": None,
+        "gpu_launches": 3 * K,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -655,7 +722,7 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cylinder_channel",
                     choices=["cylinder_channel", "kelvin_helmholtz", "taylor_green_3d",
-                             "cavity_ensemble", "closure"])
+                             "cavity_ensemble", "closure", "closure_forward"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f64"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -666,6 +733,8 @@ def main() -> None:
         run_ensemble(args)
     elif args.workload == "closure":
         run_closure(args)
+    elif args.workload == "closure_forward":
+        run_closure_forward(args)
     else:
         run_ours(args)
 
