@@ -62,7 +62,7 @@ struct StepArgs {
   int write_moments;   // 1 on the last step of an iterate call
   int path;            // kernel choice: 0 automatic, 1 direct, 2 TMA-staged (when the shape allows)
   const float* omega_field;  // per-cell om_pos (a learned closure's relaxation field), or null
-  int* status;         // bit 0 set when a non-finite density is produced
+  int* status;         // bit 0 set when a non-finite density or velocity is produced
 };
 
 enum AccMode : int { kAccNone = 0, kAccConstant = 1, kAccBoussinesq = 2 };
@@ -470,7 +470,7 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
     a.rho[c.cell] = r;
 #pragma unroll
     for (int ax = 3 - L::D; ax < 3; ++ax) a.vel[(size_t)c.cell * L::D + ax - (3 - L::D)] = u[ax];
-    if (!isfinite(r)) atomicOr(a.status, 1);
+    if (!isfinite(r) || !isfinite(uu)) atomicOr(a.status, 1);  // rho or any velocity component
   }
 
   if constexpr (NT == 1) {

@@ -139,8 +139,8 @@ LBM_API int lbm_download_fluid_f64(lbm_sim* sim, double* rho, double* vel);
  * sum of g per tracer. No reference counterpart (conservation diagnostics). Synchronous. */
 LBM_API int lbm_conservation(lbm_sim* sim, double* out, int len);
 
-/* Sets *out to 1 when a non-finite density was produced by a step that ended an iterate call
- * since the last query, else 0; clears the flag. The device-side analogue of run_sim's NaN check
+/* Sets *out to 1 when a non-finite density or velocity was produced by a step that ended an
+ * iterate call since the last query, else 0; clears the flag. The device-side analogue of run_sim's NaN check
  * (python/boltzmann/simulation.py:241-242). Synchronous. */
 LBM_API int lbm_nonfinite(lbm_sim* sim, int* out);
 
