@@ -568,8 +568,23 @@ def run_closure(args) -> None:
     e2e_s = time.perf_counter() - t1
     pipeline_s = time.perf_counter() - t0
 
-    # Tensor-core roofline of the network's forward pass on a batch of coarse states.
     nx, ny = cfg.coarse
+    # One closure application alone: the fused inference kernel on the coarse state.
+    setup_c = cl.coarse_setup(cfg)
+    flags_c = torch.tensor(setup_c.flags, device="cuda")
+    omega_c = torch.empty(nx * ny, device="cuda")
+    stream0 = torch.cuda.current_stream().cuda_stream
+    for _ in range(5):
+        cl.relaxation(net, ref.rho0, ref.vel0, flags_c, nx, ny, setup_c.tau, omega_c, stream0)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(50):
+        cl.relaxation(net, ref.rho0, ref.vel0, flags_c, nx, ny, setup_c.tau, omega_c, stream0)
+    ev1.record()
+    ev1.synchronize()
+    fused_s = ev0.elapsed_time(ev1) / 1e3 / 50
+
+    # Tensor-core roofline of the network's forward pass on a batch of coarse states.
     B = 8
     bufs = cl.Buffers(nx, ny, B, train=False)
     bufs.x.zero_()
@@ -618,6 +633,11 @@ def run_closure(args) -> None:
         },
         "closure": summary,
         "calibration": cal,
+        "fused_relaxation": {
+            "us_per_application": fused_s * 1e6,
+            "tflops": 21_312.0 * nx * ny / fused_s / 1e12,
+            "kernel": "closure_fused_kernel (features + 3 layers + tau mapping, 14x64 tiles)",
+        },
         "training": {"iters": rep.iters, "device_seconds": rep.seconds,
                      "loss_first": rep.losses[0][1], "loss_last": rep.losses[-1][1]},
         "roofline": {
@@ -687,6 +707,21 @@ def run_closure_forward(args) -> None:
     peaks, peak_kind = measured_peaks()
     peak = peaks.get("bf16_tflops", 1590.0)
     achieved = flops / (ms * 1e-3) / 1e12
+
+    # The inference kernel: features + network + relaxation rates of one 1024x512 state, fused.
+    rho = torch.tensor((1 + 0.01 * rng.normal(size=(nx, ny))).astype(np.float32), device="cuda")
+    vel = torch.tensor((0.05 * rng.normal(size=(nx, ny, 2))).astype(np.float32), device="cuda")
+    flags = torch.zeros((nx, ny), dtype=torch.int32, device="cuda")
+    omega = torch.empty(nx * ny, device="cuda")
+    for _ in range(W):
+        cl.relaxation(net, rho, vel, flags, nx, ny, 0.51, omega, stream)
+    e0.record()
+    for _ in range(K):
+        cl.relaxation(net, rho, vel, flags, nx, ny, 0.51, omega, stream)
+    e1.record()
+    e1.synchronize()
+    fused_ms = e0.elapsed_time(e1) / K
+    fused_tf = 21_312.0 * nx * ny / (fused_ms * 1e-3) / 1e12
     line = {
         "metric": "closure forward TFLOP/s",
         "value": achieved * world,
@@ -707,9 +742,12 @@ def run_closure_forward(args) -> None:
                      "frac": achieved / peak, "traffic": None,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json bf16_tflops)",
                      "kernel": "conv1_fwd + conv32_kernel (mma.sync) + conv3_fwd"},
+        "fused_relaxation": {"ms": fused_ms, "tflops": fused_tf, "frac": fused_tf / peak,
+                             "cells": nx * ny,
+                             "kernel": "closure_fused_kernel (features + 3 layers + tau)"},
         "cpu_baseline": None,
         "e2e": None,
-        "gpu_launches": 3 * K,
+        "gpu_launches": 4 * K,
         "clocks": clocks.summary(),
     }
     if rank == 0:

@@ -71,7 +71,7 @@ def build_extension(force: bool = False) -> Path:
     import pybind11
 
     src = CSRC / "pymodule.cpp"
-    deps = [src, INCLUDE / "lbm_cuda.h", LIB]
+    deps = [src, INCLUDE / "lbm_cuda.h", INCLUDE / "lbm_closure.h", LIB]
     if not force and _newer(EXT, deps):
         return EXT
     py_inc = sysconfig.get_paths()["include"]

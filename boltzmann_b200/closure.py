@@ -1,7 +1,7 @@
 """Learned subgrid closure for coarse 2D runs (D2Q9), trained on box-filtered fine runs.
 
 No counterpart in the reference. A small CNN (3x3 convolutions, 4 -> 32 -> 32 -> 1 channels,
-GELU; BF16 weights and activations, FP32 accumulation; ``csrc/closure.cu``) reads the coarse
+GELU in its tanh form; BF16 weights and activations, FP32 accumulation; ``csrc/closure.cu``) reads the coarse
 state -- (rho - 1, u_x, u_y, curl u) per cell -- and predicts the subgrid velocity scale
 sqrt(k_sgs), where k_sgs is the kinetic energy below the coarse grid that a 4x4 box filter of a
 fine run removes. Every ``every`` steps the coarse run turns the prediction into a per-cell
@@ -50,6 +50,8 @@ _SIGS = {
     "lbm_closure_sync_bf16": [_P, _P, _P],
     "lbm_closure_omega": [_P, _P, _I64, _I64, _F, _F, _F, _P, _P],
     "lbm_closure_coarsen": [_P, _P, _P, _I64, _I64, _I, _P, _P, _P, _P, _P],
+    "lbm_closure_relaxation": [_P, _P, _P, _P, _P, _I64, _I64, _P, _F, _F, _F, _P, _P],
+    "lbm_closure_status": [],
 }
 for _name, _args in _SIGS.items():
     getattr(_lib, _name).argtypes = _args
@@ -199,6 +201,32 @@ def loss_and_grad(net: Net, bufs: Buffers, target, flags, stream: int, x=None) -
     _check(_lib.lbm_closure_backward(_ptr(net.params), _ptr(net.bf16), _ptr(xs), _ptr(bufs.z1),
                                      _ptr(bufs.a1), _ptr(bufs.z2), _ptr(bufs.a2), _ptr(bufs.dy),
                                      nx, ny, batch, _ptr(bufs.grad), _ptr(bufs.ws), stream))
+
+
+def relaxation(net: Net, rho, vel, flags, nx: int, ny: int, tau0: float, omega, stream: int) -> None:
+    """The relaxation field omega [nx, ny] of a coarse state (device pointers or tensors) in one
+    kernel: features, network and the tau mapping fused (``lbm_closure_relaxation``)."""
+    rp = rho if isinstance(rho, int) else _ptr(rho)
+    vp = vel if isinstance(vel, int) else _ptr(vel)
+    nm = np.ascontiguousarray(net.norm, np.float32)
+    _check(_lib.lbm_closure_relaxation(_ptr(net.params), _ptr(net.bf16), rp, vp, _ptr(flags), nx,
+                                       ny, nm.ctypes.data_as(C.c_void_p), tau0, net.gain,
+                                       net.max_dtau, _ptr(omega), stream))
+
+
+def status() -> None:
+    """Raises if a fused relaxation kernel gave up waiting on its tensor cores (synchronous)."""
+    _check(_lib.lbm_closure_status())
+
+
+def relaxation_layered(net: Net, rho, vel, flags, bufs: Buffers, tau0: float, omega,
+                       stream: int) -> None:
+    """The same field through the layer-by-layer kernels (features, forward, omega)."""
+    nx, ny, _ = bufs.shape
+    features(rho, vel, flags, net.norm, bufs, stream)
+    forward(net, bufs, stream)
+    _check(_lib.lbm_closure_omega(_ptr(bufs.y), _ptr(flags), nx, ny, tau0, net.gain, net.max_dtau,
+                                  _ptr(omega), stream))
 
 
 class Adam:
@@ -462,18 +490,15 @@ class ClosedRun:
         self.flags = torch.tensor(np.asarray(flags, np.int32), device="cuda")
         self.steps = 0
         if net is not None:
-            self.bufs = Buffers(self.nx, self.ny, 1, train=False)
             self.omega = torch.full((self.nx * self.ny,), 1.0 / tau0, device="cuda")
             torch.cuda.synchronize()
             sim._set_omega_field(self.omega.data_ptr())
 
     def apply(self) -> None:
+        """Refresh the relaxation field from the current state (one fused kernel)."""
         rp, vp = self.sim._fluid_device()
-        features(rp, vp, self.flags, self.net.norm, self.bufs, self.stream)
-        forward(self.net, self.bufs, self.stream)
-        _check(_lib.lbm_closure_omega(_ptr(self.bufs.y), _ptr(self.flags), self.nx, self.ny,
-                                      self.tau0, self.net.gain, self.net.max_dtau,
-                                      _ptr(self.omega), self.stream))
+        relaxation(self.net, rp, vp, self.flags, self.nx, self.ny, self.tau0, self.omega,
+                   self.stream)
 
     def advance(self, steps: int) -> None:
         if steps % self.every != 0:
@@ -481,11 +506,10 @@ class ClosedRun:
         if self.net is None:
             self.sim._iterate_device(steps)
         else:
-            if self.steps == 0:
-                self.sim._iterate_device(0)  # upload + equilibrate: rho/vel valid on the device
-            for _ in range(steps // self.every):
-                self.apply()
-                self.sim._iterate_device(self.every)
+            n = self.net
+            self.sim._iterate_closure(steps, self.every, _ptr(n.params), _ptr(n.bf16),
+                                      _ptr(self.flags), n.norm, self.tau0, n.gain, n.max_dtau,
+                                      _ptr(self.omega))
         self.steps += steps
 
     def close(self) -> None:

@@ -1,7 +1,8 @@
 // Learned subgrid closure (3-layer CNN on the coarse lattice) and on-device post-processing.
 //
 // No counterpart in the reference. The network: 3x3 convolutions 4 -> 32 -> 32 -> 1 with GELU
-// after the first two layers, zero padding at the domain edges, channels-last activations.
+// (tanh form) after the first two layers, zero padding at the domain edges, channels-last
+// activations.
 //
 //   layer   forward                       backward
 //   1 (4->32)   CUDA cores (36 MAC/out)    weights: CUDA cores; no input gradient
@@ -78,14 +79,24 @@ Grid make_grid(int64_t nx, int64_t ny, int64_t batch) {
 // ---------------------------------------------------------------------------------------------
 // Scalar helpers
 
+// GELU in its tanh form, 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))), written as
+// z sigmoid(v) with v = z (a + b z^2), a = 2 sqrt(2/pi), b = 0.089430 sqrt(2/pi) (since
+// 1 + tanh(u) = 2 sigmoid(2u)); evaluated with the fast exponential and division intrinsics
+// (about 1e-6 relative, below the BF16 rounding every activation then takes). For v -> -inf the
+// quotient goes to 0, as GELU does.
+constexpr float kGeluA = 1.5957691216057308f;   // 2 sqrt(2/pi)
+constexpr float kGeluB = 0.07135481627159709f;  // 2 sqrt(2/pi) 0.044715
 __device__ __forceinline__ float gelu(float z) {
-  return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f));
+  const float v = z * fmaf(kGeluB, z * z, kGeluA);
+  return __fdividef(z, 1.0f + __expf(-v));
 }
 
+// d/dz [z sigmoid(v(z))] = s (1 + z (1 - s) v'(z)), s = sigmoid(v), v' = a + 3 b z^2.
 __device__ __forceinline__ float gelu_grad(float z) {
-  const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
-  const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
-  return cdf + z * pdf;
+  const float z2 = z * z;
+  const float v = z * fmaf(kGeluB, z2, kGeluA);
+  const float sg = __fdividef(1.0f, 1.0f + __expf(-v));
+  return sg * fmaf(z * (1.0f - sg), fmaf(3.0f * kGeluB, z2, kGeluA), 1.0f);
 }
 
 __device__ __forceinline__ float bf(bf16 v) { return __bfloat162float(v); }
@@ -220,14 +231,14 @@ __device__ __forceinline__ float vel_or_wall(const float* vel, const int32_t* fl
   return (flags[cell] & 1) ? 0.0f : vel[(b * n + cell) * 2 + c];
 }
 
-__global__ void features_kernel(const float* __restrict__ rho, const float* __restrict__ vel,
-                                const int32_t* __restrict__ flags, int64_t nx, int64_t ny,
-                                int64_t batch, Norm norm, bf16* __restrict__ x_out) {
+// The four BF16 features of cell (x, y) of batch entry b, packed in two words (0 on walls).
+__device__ __forceinline__ uint2 cell_features(const float* __restrict__ rho,
+                                               const float* __restrict__ vel,
+                                               const int32_t* __restrict__ flags, int64_t nx,
+                                               int64_t ny, int64_t b, int64_t x, int64_t y,
+                                               const Norm& norm) {
   const int64_t n = nx * ny;
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n * batch) return;
-  const int64_t b = i / n, cell = i - b * n;
-  const int64_t x = cell / ny, y = cell - x * ny;
+  const int64_t cell = x * ny + y, i = b * n + cell;
   uint2 packed = make_uint2(0, 0);
   if (!(flags[cell] & 1)) {
     const int64_t xm = x > 0 ? x - 1 : x, xp = x < nx - 1 ? x + 1 : x;
@@ -246,7 +257,18 @@ __global__ void features_kernel(const float* __restrict__ rho, const float* __re
     packed.x = (uint32_t)__bfloat16_as_ushort(h[0]) | ((uint32_t)__bfloat16_as_ushort(h[1]) << 16);
     packed.y = (uint32_t)__bfloat16_as_ushort(h[2]) | ((uint32_t)__bfloat16_as_ushort(h[3]) << 16);
   }
-  reinterpret_cast<uint2*>(x_out)[i] = packed;
+  return packed;
+}
+
+__global__ void features_kernel(const float* __restrict__ rho, const float* __restrict__ vel,
+                                const int32_t* __restrict__ flags, int64_t nx, int64_t ny,
+                                int64_t batch, Norm norm, bf16* __restrict__ x_out) {
+  const int64_t n = nx * ny;
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n * batch) return;
+  const int64_t b = i / n, cell = i - b * n;
+  const int64_t x = cell / ny, y = cell - x * ny;
+  reinterpret_cast<uint2*>(x_out)[i] = cell_features(rho, vel, flags, nx, ny, b, x, y, norm);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -772,6 +794,432 @@ __global__ void loss_final_kernel(const double* __restrict__ partial, int blocks
 }
 
 // ---------------------------------------------------------------------------------------------
+// Blackwell tensor cores (tcgen05): MMAs issued by one thread on shared-memory operands,
+// accumulators in tensor memory (TMEM), completion signalled through an mbarrier.
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor, K-major without swizzle: rows (M or N) 16 bytes apart inside a
+// group of 8 rows, `sbo` bytes between groups of 8 rows, `lbo` bytes between the two 8-element K
+// halves of one MMA. Descriptor version 1 (sm_100).
+__device__ __forceinline__ uint64_t umma_desc(unsigned start, unsigned lbo, unsigned sbo) {
+  return (uint64_t)((start >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: BF16 A and B, FP32 accumulator, both K-major, M x N.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int m, int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, bool accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate ? 1u : 0u), "r"(0u), "r"(0u), "r"(0u),
+      "r"(0u));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_addr(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// 32 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+      "%30, %31}, [%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+        "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+        "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+constexpr unsigned kClosureSpinLimit = 1u << 22;
+
+__device__ __forceinline__ void cl_mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+}
+
+// Bounded wait for the phase with the given parity; false on timeout.
+__device__ __forceinline__ bool cl_mbar_wait(uint64_t* bar, unsigned parity) {
+  const unsigned addr = smem_addr(bar);
+  for (unsigned i = 0; i < kClosureSpinLimit; ++i) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// Set (bit 0) when a closure kernel gave up waiting for its tensor-core work; read and cleared
+// by lbm_closure_status.
+__device__ int g_closure_status;
+
+// ---------------------------------------------------------------------------------------------
+// Inference in one pass: features, the three layers and the relaxation field for a tile of
+// kFR x kFC output cells, every intermediate in shared memory (~213 KB, one CTA of 16 warps per
+// SM). The raw fields of the tile's neighbourhood are staged first with coalesced loads. Each
+// layer is evaluated on its own halo-extended region -- layer 3 reads layer 2 one cell around
+// the tile, layer 2 reads layer 1 two cells around, layer 1 reads the features three cells
+// around -- and outside the domain every layer's output is 0, the zero padding the
+// layer-by-layer kernels apply. All three layers run on tensor cores (mma.sync BF16 -> FP32):
+// layer 1 with K = 48 (9 taps x 4 channels, zero-padded from 36), layer 2 with K = 288, layer 3
+// with K = 288 and N = 8 (one real output column). A warp's
+// 16-row MMA tile is any 16 consecutive cells of a region in row-major order (ldmatrix takes one
+// row address per lane), so the regions need not be multiples of 16 wide.
+
+constexpr int kFR = 14, kFC = 64;               // output tile
+constexpr int kA2R = kFR + 2, kA2C = kFC + 2;  // layer-2 region
+constexpr int kA1R = kFR + 4, kA1C = kFC + 4;  // layer-1 region
+constexpr int kXR = kFR + 6, kXC = kFC + 6;    // feature region
+constexpr int kRawR = kFR + 8, kRawC = kFC + 8;  // raw fields (features read one cell around)
+constexpr int kW1S = 56;                        // shared-memory BF16 per layer-1 weight row
+constexpr int kFusedThreads = 512;
+// Layer 1's output is stored "chunk-major" for the tensor-core descriptors: plane k (channels
+// 8k .. 8k+7) holds 16 bytes per cell, cells in row-major order of the layer-1 region
+// (kA1R x kA1C), padded so that every shifted 128-cell block stays inside the plane.
+constexpr int kA1Pad = 1296;                    // >= 69 + 9 * 128 + 69 cells
+constexpr int kL2Blocks = 9;                    // 128-cell blocks covering the layer-2 region
+constexpr int kL2First = kA1C + 1;              // layer-1 flat index of layer-2 cell (0, 0)
+constexpr size_t kFusedOffA1 = (size_t)kXR * kXC * 8;
+constexpr size_t kFusedOffA2 = kFusedOffA1 + (size_t)4 * kA1Pad * 16;
+constexpr size_t kFusedOffW1 = kFusedOffA2 + (size_t)kA2R * kA2C * kCS * 2;
+constexpr size_t kFusedOffW2 = kFusedOffW1 + (size_t)C * kW1S * 2;
+constexpr size_t kFusedOffW3 = kFusedOffW2 + (size_t)36 * C * 16;  // 36 K-chunks x 32 rows x 16 B
+constexpr size_t kFusedOffB = kFusedOffW3 + (size_t)9 * C * 4;
+constexpr size_t kFusedOffBar = kFusedOffB + (size_t)2 * C * 4;    // mbarrier + TMEM address
+constexpr size_t kFusedSmem = kFusedOffBar + 16;
+static_assert(kL2First + kL2Blocks * 128 + kA1C + 1 <= kA1Pad, "layer-1 planes too short");
+static_assert(kL2First + kL2Blocks * 128 > (kA2R * kA1C) + kA2C, "blocks do not cover layer 2");
+constexpr int kTmemCols = 512;  // 9 accumulators of 32 FP32 columns (power of two >= 288)
+static_assert((size_t)kRawR * kRawC * 16 <= (size_t)kA2R * kA2C * kCS * 2,
+              "the staged raw fields must fit in the layer-2 area");
+
+struct FusedArgs {
+  const float* params;
+  const bf16* wb;
+  const float* rho;
+  const float* vel;
+  const int32_t* flags;
+  int64_t nx, ny;
+  Norm norm;
+  float tau0, gain, max_dtau;
+  float* omega;
+  int tiles_x, tiles_y;
+};
+
+__global__ void __launch_bounds__(kFusedThreads, 1)
+    closure_fused_kernel(const __grid_constant__ FusedArgs f) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint32_t* xs = reinterpret_cast<uint32_t*>(smem_raw);  // [cell][2 words]: channels 0-1, 2-3
+  unsigned char* a1c = smem_raw + kFusedOffA1;  // [4 planes][kA1Pad cells][16 B]
+  bf16* a2s = reinterpret_cast<bf16*>(smem_raw + kFusedOffA2);
+  bf16* w1s = reinterpret_cast<bf16*>(smem_raw + kFusedOffW1);
+  unsigned char* w2c = smem_raw + kFusedOffW2;  // [36 K-chunks][32 out channels][16 B]
+  bf16* w3b = reinterpret_cast<bf16*>(smem_raw + kFusedOffW3);  // [9][32]
+  float* bs = reinterpret_cast<float*>(smem_raw + kFusedOffB);  // b1 [32], b2 [32]
+  uint64_t* mma_done = reinterpret_cast<uint64_t*>(smem_raw + kFusedOffBar);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem_raw + kFusedOffBar + 8);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gq = lane >> 2, tq = lane & 3, mi = lane >> 3, rr = lane & 7;
+  constexpr int kWarps = kFusedThreads / 32;
+
+  for (int i = threadIdx.x; i < C * kW1S; i += blockDim.x) {
+    const int co = i / kW1S, k = i - co * kW1S;
+    w1s[i] = k < 36 ? f.wb[LBM_CLOSURE_OFF_W1 + co * 36 + k] : __float2bfloat16(0.0f);
+  }
+  // Layer-2 weights as the MMA's B operand: K-chunk kk (k = 8 kk .. 8 kk + 7, k = tap*32 + ci)
+  // of output channel co at (kk * 32 + co) * 16 bytes.
+  for (int i = threadIdx.x; i < 36 * C; i += blockDim.x) {
+    const int kk = i / C, co = i - kk * C;
+    *reinterpret_cast<uint4*>(w2c + (size_t)i * 16) =
+        __ldg(reinterpret_cast<const uint4*>(f.wb + LBM_CLOSURE_OFF_W2 + co * 288 + kk * 8));
+  }
+  for (int i = threadIdx.x; i < 9 * C; i += blockDim.x) w3b[i] = f.wb[LBM_CLOSURE_OFF_W3 + i];
+  for (int i = threadIdx.x; i < 2 * C; i += blockDim.x)
+    bs[i] = f.params[i < C ? LBM_CLOSURE_OFF_B1 + i : LBM_CLOSURE_OFF_B2 + i - C];
+  const float b3 = f.params[LBM_CLOSURE_OFF_B3];
+  // Padding cells of the layer-1 planes feed only discarded rows; keep them finite.
+  for (int i = threadIdx.x; i < 4 * kA1Pad; i += blockDim.x) {
+    if (i % kA1Pad >= kA1R * kA1C)
+      *reinterpret_cast<uint4*>(a1c + (size_t)i * 16) = make_uint4(0, 0, 0, 0);
+  }
+  if (threadIdx.x == 0) {
+    cl_mbar_init(mma_done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t idesc = umma_idesc_bf16(128, 32);
+  const unsigned a1c_addr = smem_addr(a1c), w2c_addr = smem_addr(w2c);
+  bool healthy = true;
+  unsigned phase = 0;
+
+  const int ntiles = f.tiles_x * f.tiles_y;
+  for (int t = blockIdx.x; t < ntiles && healthy; t += gridDim.x) {
+    const int64_t x0 = (int64_t)(t / f.tiles_y) * kFR, y0 = (int64_t)(t % f.tiles_y) * kFC;
+    tc_fence_before();
+    __syncthreads();  // the previous tile is done with every region and every TMEM column
+    tc_fence_after();
+
+    // Raw fields on [x0 - 4, x0 + kFR + 4) x [y0 - 4, y0 + kFC + 4), staged with coalesced loads
+    // into the layer-2 area (free until layer 2 runs); velocities on walls read as 0.
+    float* raw_rho = reinterpret_cast<float*>(a2s);
+    float2* raw_vel = reinterpret_cast<float2*>(raw_rho + kRawR * kRawC);
+    int* raw_flag = reinterpret_cast<int*>(raw_vel + kRawR * kRawC);
+    for (int i = threadIdx.x; i < kRawR * kRawC; i += blockDim.x) {
+      const int r = i / kRawC, c = i - r * kRawC;
+      const int64_t x = x0 - 4 + r, y = y0 - 4 + c;
+      float rv = 0.0f;
+      float2 vv = make_float2(0.0f, 0.0f);
+      int fl = 0;
+      if (x >= 0 && x < f.nx && y >= 0 && y < f.ny) {
+        const int64_t cell = x * f.ny + y;
+        rv = f.rho[cell];
+        vv = *reinterpret_cast<const float2*>(f.vel + 2 * cell);
+        fl = f.flags[cell];
+      }
+      raw_rho[i] = rv;
+      raw_vel[i] = vv;
+      raw_flag[i] = fl;
+    }
+    __syncthreads();
+    // Features on [x0 - 3, x0 + kFR + 3) x [y0 - 3, y0 + kFC + 3), the arithmetic of
+    // cell_features (np.gradient edges, walls at rest, normalise, BF16) on the staged fields.
+    for (int i = threadIdx.x; i < kXR * kXC; i += blockDim.x) {
+      const int r = i / kXC, c = i - r * kXC;
+      const int64_t x = x0 - 3 + r, y = y0 - 3 + c;
+      uint2 packed = make_uint2(0, 0);
+      const int ri = (r + 1) * kRawC + c + 1;  // this cell in the raw region
+      if (x >= 0 && x < f.nx && y >= 0 && y < f.ny && !(raw_flag[ri] & 1)) {
+        const int im = x > 0 ? ri - kRawC : ri, ip = x < f.nx - 1 ? ri + kRawC : ri;
+        const int jm = y > 0 ? ri - 1 : ri, jp = y < f.ny - 1 ? ri + 1 : ri;
+        auto vx = [&](int k) { return (raw_flag[k] & 1) ? 0.0f : raw_vel[k].x; };
+        auto vy = [&](int k) { return (raw_flag[k] & 1) ? 0.0f : raw_vel[k].y; };
+        const float dux_dy = np_gradient(vx(jm), raw_vel[ri].x, vx(jp), y, f.ny);
+        const float duy_dx = np_gradient(vy(im), raw_vel[ri].y, vy(ip), x, f.nx);
+        const float v[4] = {__fsub_rn(raw_rho[ri], 1.0f), raw_vel[ri].x, raw_vel[ri].y,
+                            __fsub_rn(dux_dy, duy_dx)};
+        bf16 h[4];
+#pragma unroll
+        for (int ch = 0; ch < 4; ++ch)
+          h[ch] = to_bf(__fmul_rn(__fsub_rn(v[ch], f.norm.mean[ch]), f.norm.inv_std[ch]));
+        packed.x = (uint32_t)__bfloat16_as_ushort(h[0]) | ((uint32_t)__bfloat16_as_ushort(h[1]) << 16);
+        packed.y = (uint32_t)__bfloat16_as_ushort(h[2]) | ((uint32_t)__bfloat16_as_ushort(h[3]) << 16);
+      }
+      xs[2 * i] = packed.x;
+      xs[2 * i + 1] = packed.y;
+    }
+    __syncthreads();
+
+    // Layer 1 on [x0 - 2, ..) x [y0 - 2, ..): A fragments gathered from the features by tap.
+    constexpr int n1 = kA1R * kA1C;
+    for (int mt = warp; mt * 16 < n1; mt += kWarps) {
+      int rq[2], cq[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int q = min(mt * 16 + gq + 8 * h, n1 - 1);
+        rq[h] = q / kA1C;
+        cq[h] = q - rq[h] * kA1C;
+      }
+      float acc[4][4];
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[nt][e] = 0.0f;
+#pragma unroll
+      for (int kk = 0; kk < 3; ++kk) {
+        uint32_t a[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int h = e & 1, k = kk * 16 + 2 * tq + (e >> 1) * 8, tap = k >> 2;
+          a[e] = 0u;
+          if (tap < 9) {
+            const int xi = (rq[h] + 1 + tap / 3 - 1) * kXC + cq[h] + 1 + tap % 3 - 1;
+            a[e] = xs[2 * xi + ((k & 3) >> 1)];
+          }
+        }
+        uint32_t bfr[4][2];
+#pragma unroll
+        for (int np = 0; np < 2; ++np) {
+          uint32_t r4[4];
+          ldsm_x4(r4, w1s + ((2 * np + (mi >> 1)) * 8 + rr) * kW1S + kk * 16 + (mi & 1) * 8);
+          bfr[2 * np][0] = r4[0];
+          bfr[2 * np][1] = r4[1];
+          bfr[2 * np + 1][0] = r4[2];
+          bfr[2 * np + 1][1] = r4[3];
+        }
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) mma_bf16(acc[nt], a, bfr[nt][0], bfr[nt][1]);
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int q = mt * 16 + gq + 8 * h;
+        if (q >= n1) continue;
+        const int64_t x = x0 - 2 + rq[h], y = y0 - 2 + cq[h];
+        const bool inside = x >= 0 && x < f.nx && y >= 0 && y < f.ny;
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          const int ch = nt * 8 + 2 * tq;
+          __nv_bfloat162 o;
+          o.x = to_bf(inside ? gelu(acc[nt][2 * h] + bs[ch]) : 0.0f);
+          o.y = to_bf(inside ? gelu(acc[nt][2 * h + 1] + bs[ch + 1]) : 0.0f);
+          *reinterpret_cast<__nv_bfloat162*>(a1c + ((size_t)nt * kA1Pad + q) * 16 + tq * 4) = o;
+        }
+      }
+    }
+    __syncthreads();
+
+    // Layer 2 on tcgen05: nine blocks of 128 consecutive layer-1 cells (flat index from the
+    // layer-1 cell of layer-2 cell (0, 0)), each an M = 128, N = 32, K = 288 product into its own
+    // 32 TMEM columns. Tap (dx, dy) reads the block shifted by dx * kA1C + dy cells: with the
+    // chunk-major planes that is an offset of the descriptor's start address (16 bytes a cell).
+    // Rows that fall on the region's first or last column are computed and discarded.
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // layer 1 visible to the MMAs
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tc_fence_after();
+      // K-slice outer, block inner: consecutive MMAs accumulate into different TMEM columns.
+#pragma unroll 1
+      for (int tap = 0; tap < 9; ++tap) {
+        const int off = (tap / 3 - 1) * kA1C + (tap % 3 - 1);
+#pragma unroll
+        for (int kc = 0; kc < 2; ++kc) {
+          const int sidx = tap * 2 + kc;
+          const uint64_t bdesc = umma_desc(w2c_addr + (unsigned)(sidx * 1024), C * 16, 128);
+          const unsigned a_base = a1c_addr + (unsigned)((2 * kc * kA1Pad + kL2First + off) * 16);
+#pragma unroll
+          for (int m = 0; m < kL2Blocks; ++m)
+            umma_bf16(tmem + (uint32_t)(m * 32),
+                      umma_desc(a_base + (unsigned)(m * 128 * 16), kA1Pad * 16, 128), bdesc,
+                      idesc, sidx != 0);
+        }
+      }
+      umma_commit(mma_done);
+    }
+    const bool got = cl_mbar_wait(mma_done, phase);
+    phase ^= 1u;
+    if (!__syncthreads_and(got)) {
+      healthy = false;
+      break;
+    }
+    tc_fence_after();
+    // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its sub-partition) of blocks
+    // w / 4, w / 4 + 4, w / 4 + 8; one thread per cell, its 32 channels in registers.
+    for (int m = warp >> 2; m < kL2Blocks; m += kWarps / 4) {
+      const int sp = warp & 3;
+      uint32_t r32[32];
+      tmem_ld32(tmem + ((uint32_t)(32 * sp) << 16) + (uint32_t)(m * 32), r32);
+      const int p = kL2First + 128 * m + 32 * sp + lane;  // layer-1 flat index of this row
+      const int r = p / kA1C - 1, c = p % kA1C - 1;      // layer-2 region coordinates
+      if (r < 0 || r >= kA2R || c < 0 || c >= kA2C) continue;
+      const int64_t x = x0 - 1 + r, y = y0 - 1 + c;
+      const bool inside = x >= 0 && x < f.nx && y >= 0 && y < f.ny;
+      uint32_t packed[C / 2];
+#pragma unroll
+      for (int ch = 0; ch < C; ch += 2) {
+        const float v0 = inside ? gelu(__uint_as_float(r32[ch]) + bs[C + ch]) : 0.0f;
+        const float v1 = inside ? gelu(__uint_as_float(r32[ch + 1]) + bs[C + ch + 1]) : 0.0f;
+        packed[ch / 2] = (uint32_t)__bfloat16_as_ushort(to_bf(v0)) |
+                         ((uint32_t)__bfloat16_as_ushort(to_bf(v1)) << 16);
+      }
+      uint4* dst = reinterpret_cast<uint4*>(a2s + (r * kA2C + c) * kCS);
+#pragma unroll
+      for (int q = 0; q < C / 8; ++q)
+        dst[q] = make_uint4(packed[4 * q], packed[4 * q + 1], packed[4 * q + 2], packed[4 * q + 3]);
+    }
+    __syncthreads();
+
+    // Layer 3 on tensor cores (N = 8 with only column 0 carrying w3; K = 288) and the relaxation
+    // rate (the mapping of omega_kernel) on the output tile: 16 cells of one tile row per MMA tile.
+    constexpr int n3 = kFR * kFC;
+    for (int mt = warp; mt * 16 < n3; mt += kWarps) {
+      const int j = (lane & 7) + 8 * ((lane >> 3) & 1);
+      const int qa = mt * 16 + j;
+      const int ra = qa / kFC, ca = qa - ra * kFC;
+      float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll 1
+      for (int tap = 0; tap < 9; ++tap) {
+        const int dx = tap / 3 - 1, dy = tap % 3 - 1;
+        const bf16* arow = a2s + ((ra + 1 + dx) * kA2C + ca + 1 + dy) * kCS + 8 * (lane >> 4);
+#pragma unroll
+        for (int kc = 0; kc < 2; ++kc) {
+          uint32_t a[4];
+          ldsm_x4(a, arow + kc * 16);
+          // B column 0 = w3[tap][kc*16 + k]; lanes of the other columns hold zeros.
+          uint32_t b0 = 0u, b1 = 0u;
+          if (gq == 0) {
+            const int k0 = tap * C + kc * 16 + 2 * tq;
+            b0 = *reinterpret_cast<const uint32_t*>(w3b + k0);
+            b1 = *reinterpret_cast<const uint32_t*>(w3b + k0 + 8);
+          }
+          mma_bf16(acc, a, b0, b1);
+        }
+      }
+      if (tq == 0) {  // column 0: rows gq and gq + 8 of this tile
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int q = mt * 16 + gq + 8 * h;
+          const int r = q / kFC, c = q - r * kFC;
+          const int64_t x = x0 + r, y = y0 + c;
+          if (x >= f.nx || y >= f.ny) continue;
+          const float yv = acc[2 * h] + b3;
+          const int64_t cell = x * f.ny + y;
+          float tau = f.tau0;
+          if (fluid_cell(f.flags[cell])) tau += fminf(f.max_dtau, f.gain * fmaxf(yv, 0.0f));
+          f.omega[cell] = 1.0f / tau;
+        }
+      }
+    }
+  }
+  if (!healthy) {
+    if (threadIdx.x == 0) {
+      atomicOr(&g_closure_status, 1);
+      cl_mbar_wait(mma_done, phase ^ 1u);  // give MMAs still in flight a bounded chance to end
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
+                 : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
 // Optimiser, relaxation field, coarsening
 
 __global__ void adam_kernel(float* __restrict__ p, bf16* __restrict__ pb, const float* __restrict__ g,
@@ -1048,6 +1496,55 @@ int lbm_closure_omega(const float* y, const int32_t* flags, int64_t nx, int64_t 
                                                                          gain, max_dtau, omega);
   CL_CUDA(cudaGetLastError());
   return LBM_OK;
+}
+
+int lbm_closure_relaxation(const float* params, const uint16_t* params_bf16, const float* rho,
+                           const float* vel, const int32_t* flags, int64_t nx, int64_t ny,
+                           const float* norm, float tau0, float gain, float max_dtau,
+                           float* omega, void* stream) {
+  if (!params || !params_bf16 || !rho || !vel || !flags || !norm || !omega || nx < 2 || ny < 2 ||
+      !(tau0 > 0.5f) || !(max_dtau >= 0.0f))
+    return fail(LBM_ERR_ARGUMENT, "closure relaxation: bad arguments");
+  if (!aligned16(params_bf16))
+    return fail(LBM_ERR_ARGUMENT, "closure relaxation: params_bf16 must be 16-byte aligned");
+  static thread_local bool configured = false;
+  if (!configured) {
+    if (int rc = set_smem((const void*)closure_fused_kernel, kFusedSmem)) return rc;
+    configured = true;
+  }
+  FusedArgs fa;
+  fa.params = params;
+  fa.wb = reinterpret_cast<const bf16*>(params_bf16);
+  fa.rho = rho;
+  fa.vel = vel;
+  fa.flags = flags;
+  fa.nx = nx;
+  fa.ny = ny;
+  for (int c = 0; c < 4; ++c) {
+    fa.norm.mean[c] = norm[c];
+    fa.norm.inv_std[c] = norm[4 + c];
+  }
+  fa.tau0 = tau0;
+  fa.gain = gain;
+  fa.max_dtau = max_dtau;
+  fa.omega = omega;
+  fa.tiles_x = (int)((nx + kFR - 1) / kFR);
+  fa.tiles_y = (int)((ny + kFC - 1) / kFC);
+  const int64_t ntiles = (int64_t)fa.tiles_x * fa.tiles_y;
+  const int grid = (int)std::min<int64_t>(ntiles, (int64_t)device_sms());
+  closure_fused_kernel<<<grid, kFusedThreads, kFusedSmem, (cudaStream_t)stream>>>(fa);
+  CL_CUDA(cudaGetLastError());
+  return LBM_OK;
+}
+
+int lbm_closure_status(void) {
+  int word = 0;
+  CL_CUDA(cudaMemcpyFromSymbol(&word, g_closure_status, sizeof(int)));
+  if (word == 0) return LBM_OK;
+  const int zero = 0;
+  CL_CUDA(cudaMemcpyToSymbol(g_closure_status, &zero, sizeof(int)));
+  return fail(LBM_ERR_STATE,
+              "closure relaxation: a kernel gave up waiting for its tensor-core products");
 }
 
 int lbm_closure_coarsen(const float* rho, const float* vel, const float* c, int64_t nx, int64_t ny,

@@ -21,6 +21,7 @@
 #include <string>
 #include <vector>
 
+#include "lbm_closure.h"
 #include "lbm_cuda.h"
 
 namespace py = pybind11;
@@ -524,6 +525,40 @@ PYBIND11_MODULE(boltzmann, m) {
              // Per-cell omega+ (device address of N floats, kept alive by the caller); 0 clears it.
              std::lock_guard<std::recursive_mutex> lock(s.st->mu);
              check(lbm_set_omega_field(s.st->h, reinterpret_cast<const float*>(field)));
+           })
+      .def("_iterate_closure",
+           [](Simulation& s, int64_t iters, int64_t every, uintptr_t params, uintptr_t params_bf16,
+              uintptr_t flags, py::array_t<float, py::array::c_style | py::array::forcecast> norm,
+              float tau0, float gain, float max_dtau, uintptr_t omega) {
+             // Steps of a 2D run whose relaxation field the learned closure refreshes every
+             // `every` steps (lbm_closure_relaxation on the simulation's stream, then `every`
+             // steps), the whole loop issued from here so the GPU never waits on Python.
+             // Pointers are device addresses the caller keeps alive; omega stays installed as the
+             // simulation's field.
+             SimState& st = *s.st;
+             if (st.dim != 2 || st.q != 9) throw py::value_error("the closure drives D2Q9 runs");
+             if (every <= 0 || every % 2 != 0 || iters % every != 0)
+               throw py::value_error("iters must be a multiple of an even closure interval");
+             if (norm.size() != 8) throw py::value_error("norm must hold 8 floats");
+             std::array<float, 8> nm;
+             std::copy(norm.data(), norm.data() + 8, nm.begin());
+             py::gil_scoped_release nogil;
+             std::lock_guard<std::recursive_mutex> lock(st.mu);
+             st.prepare();
+             void *rho = nullptr, *vel = nullptr, *stream = nullptr;
+             check(lbm_fluid_device(st.h, &rho, &vel));
+             check(lbm_stream(st.h, &stream));
+             float* om = reinterpret_cast<float*>(omega);
+             check(lbm_set_omega_field(st.h, om));
+             for (int64_t done = 0; done < iters; done += every) {
+               check(lbm_closure_relaxation(
+                   reinterpret_cast<const float*>(params),
+                   reinterpret_cast<const uint16_t*>(params_bf16), static_cast<const float*>(rho),
+                   static_cast<const float*>(vel), reinterpret_cast<const int32_t*>(flags),
+                   st.counts[0], st.counts[1], nm.data(), tau0, gain, max_dtau, om, stream));
+               check(lbm_iterate(st.h, every));
+               st.iteration += (uint64_t)every;
+             }
            })
       .def("_synchronize", [](const Simulation& s) { check(lbm_synchronize(s.st->h)); })
       .def("_stream", [](const Simulation& s) {

@@ -4,8 +4,8 @@
  * (python/boltzmann/utils/postproc.py:12-83) is numpy on the host.
  *
  * The closure is a 3-layer CNN on the coarse lattice: 3x3 convolutions with 4 -> 32 -> 32 -> 1
- * channels, GELU after the first two, zero padding at the domain edges. Inputs per cell are
- * (rho - 1, u_x, u_y, curl u), normalised and stored as BF16; weights are BF16 copies of an FP32
+ * channels, GELU (tanh form) after the first two, zero padding at the domain edges. Inputs per
+ * cell are (rho - 1, u_x, u_y, curl u), normalised and stored as BF16; weights are BF16 copies of an FP32
  * master vector; every product sum accumulates in FP32 (tensor cores for the 32 -> 32 layer, in
  * both directions). Its output, times a gain, is a per-cell relaxation-time correction that
  * lbm_set_omega_field() hands to the stencil.
@@ -110,6 +110,23 @@ LBM_API int lbm_closure_sync_bf16(const float* params, uint16_t* params_bf16, vo
  * 1 / tau0 elsewhere (the stencil relaxes fixed cells with 1 regardless). */
 LBM_API int lbm_closure_omega(const float* y, const int32_t* flags, int64_t nx, int64_t ny,
                               float tau0, float gain, float max_dtau, float* omega, void* stream);
+
+/* Inference in one kernel: the relaxation field omega [nx][ny] of lbm_closure_omega, computed
+ * from the coarse state (rho [nx][ny], vel [nx][ny][2], flags) through the features and the three
+ * layers without any intermediate array in global memory (each tile recomputes its halo in shared
+ * memory; all three layers on tensor cores, the 32 -> 32 layer as tcgen05 MMAs with TMEM
+ * accumulators). Equal to lbm_closure_features + lbm_closure_forward +
+ * lbm_closure_omega up to the FP32 summation order of layers 1 and 3. `norm` is a host array of
+ * 8 floats. */
+LBM_API int lbm_closure_relaxation(const float* params, const uint16_t* params_bf16,
+                                   const float* rho, const float* vel, const int32_t* flags,
+                                   int64_t nx, int64_t ny, const float* norm, float tau0,
+                                   float gain, float max_dtau, float* omega, void* stream);
+
+/* LBM_OK, or LBM_ERR_STATE when a lbm_closure_relaxation kernel on the current device gave up
+ * waiting for its tensor-core products (bounded wait) since the last call; its omega is then
+ * incomplete. Synchronous; clears the condition. */
+LBM_API int lbm_closure_status(void);
 
 /* Box filter of a fine state onto the coarse lattice (factor f, nx and ny multiples of f):
  * rho_c, vel_c ([nx/f][ny/f], [..][2]) and c_c (if c != NULL) are block means; sgs gets the

@@ -7,8 +7,8 @@ the checker of the CUDA kernels in ``boltzmann_b200/csrc/closure.cu``; the produ
   (``calc_vmag``, ``calc_curl``: ``np.gradient`` derivatives, d(u_x)/dy - d(u_y)/dx in 2D).
   Pinned by ``tests/golden/postproc.npz``, made by the reference's own functions.
 * ``forward`` / ``backward`` restate the network (4 -> 32 -> 32 -> 1 channels, 3x3 convolutions,
-  zero padding, exact GELU) in float64 numpy, with the BF16 roundings the CUDA kernels apply
-  (weights, activations, pre-activation gradients; round to nearest even). With ``exact=True`` the
+  zero padding, GELU in its tanh form) in float64 numpy, with the BF16 roundings the CUDA kernels
+  apply (weights, activations, pre-activation gradients; round to nearest even). With ``exact=True`` the
   roundings are skipped, and the tests pin ``backward`` against finite differences of
   ``forward`` -- the reference has no closure, so that is what pins the gradients.
 
@@ -19,7 +19,6 @@ w3 [9][32], b3 [1]; tap = 3 (dx + 1) + (dy + 1), x the slow axis.
 from __future__ import annotations
 
 import numpy as np
-from scipy.special import erf
 
 C = 32
 OFF = {"w1": 0, "b1": 1152, "w2": 1184, "b2": 10400, "w3": 10432, "b3": 10720}
@@ -124,12 +123,17 @@ def coarsen(rho, vel, c, f: int):
 # ---- network -------------------------------------------------------------------------------
 
 
+_C = np.sqrt(2.0 / np.pi)
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    """GELU in its tanh form, 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))."""
+    return 0.5 * z * (1.0 + np.tanh(_C * (z + 0.044715 * z**3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(_C * (z + 0.044715 * z**3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * _C * (1.0 + 3 * 0.044715 * z**2)
 
 
 def _pad(a):

@@ -248,3 +248,37 @@ def test_omega_field_is_local(torch):
     np.testing.assert_array_equal(a.fluid.vel[:19], b.fluid.vel[:19])
     assert not np.array_equal(a.fluid.vel[30:], b.fluid.vel[30:])
     a._set_omega_field(0)
+
+
+# Partial tiles in both directions (tiles are 14 x 64 output cells), an exact tile, a tiny domain,
+# and the full coarse lattice of the closure experiment.
+FUSED_SHAPES = [(30, 70), (14, 64), (5, 9), (1024, 512)]
+
+
+@pytest.mark.parametrize("nx,ny", FUSED_SHAPES)
+def test_fused_relaxation_matches_layered_kernels(torch, cl, nx, ny):
+    """lbm_closure_relaxation (features, three layers and the tau mapping in one kernel, halos
+    recomputed per tile, layer 2 on tcgen05) against the layer-by-layer kernels on the same state.
+    Every layer sums in a different order there (FP32 FMAs, warp MMAs), so BF16 activations may
+    differ by one unit on rounding boundaries; the relaxation rates agree to 1e-4 relative."""
+    rho, vel, flags, norm = _inputs(11, 1, nx, ny)
+    net = cl.Net(co.init_params(4), norm, gain=0.02, max_dtau=0.05)
+    flags_t = torch.tensor(flags, device="cuda")
+    r = torch.tensor(rho[0], device="cuda")
+    v = torch.tensor(vel[0], device="cuda")
+    fused = torch.full((nx * ny,), float("nan"), device="cuda")
+    layered = torch.full((nx * ny,), float("nan"), device="cuda")
+    bufs = cl.Buffers(nx, ny, 1, train=False)
+    for _ in range(2):  # two calls in a row: no state carried between them
+        cl.relaxation(net, r, v, flags_t, nx, ny, 0.51, fused, 0)
+    cl.relaxation_layered(net, r, v, flags_t, bufs, 0.51, layered, 0)
+    torch.cuda.synchronize()
+    cl.status()
+    a, b = fused.cpu().numpy(), layered.cpu().numpy()
+    assert np.isfinite(a).all()
+    assert np.abs(a - b).max() <= 1e-4 * np.abs(b).max()
+    assert np.mean(a == b) > 0.9
+    fixed_or_wall = (flags.reshape(-1) & 7) != 0
+    assert (a[fixed_or_wall] == np.float32(1.0) / np.float32(0.51)).all()
+    # the network's output really varies the rate inside the fluid
+    assert np.ptp(a[~fixed_or_wall]) > 1e-3
