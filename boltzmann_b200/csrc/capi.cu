@@ -265,11 +265,14 @@ int lbm_add_coupling(lbm_sim* sim, int tracer, float alpha, float c0, const floa
 int lbm_upload_flags(lbm_sim* sim, const int32_t* flags) {
   if (int rc = activate(sim)) return rc;
   if (flags == nullptr) return fail(LBM_ERR_ARGUMENT, "null flags");
-  // Only bits 0-3 are read by the kernels (WALL, FIXED_FLUID_*, FIXED_SCALAR_VALUE).
-  std::vector<uint8_t> low((size_t)sim->n);
-  for (int64_t i = 0; i < sim->n; ++i) low[(size_t)i] = (uint8_t)(flags[i] & 0xF);
-  LBM_CUDA(cudaMemcpyAsync(sim->flags, low.data(), (size_t)sim->n, cudaMemcpyHostToDevice,
+  // Only bits 0-3 are read by the kernels (WALL, FIXED_FLUID_*, FIXED_SCALAR_VALUE): the int32
+  // array goes over as it is (one DMA from the caller's buffer) and is narrowed on the device.
+  int32_t* tmp = nullptr;
+  LBM_CUDA(cudaMallocAsync((void**)&tmp, (size_t)sim->n * sizeof(int32_t), sim->stream));
+  LBM_CUDA(cudaMemcpyAsync(tmp, flags, (size_t)sim->n * sizeof(int32_t), cudaMemcpyHostToDevice,
                            sim->stream));
+  LBM_CUDA(lbm::flags_to_u8(tmp, static_cast<uint8_t*>(sim->flags), sim->n, sim->stream));
+  LBM_CUDA(cudaFreeAsync(tmp, sim->stream));
   LBM_CUDA(cudaStreamSynchronize(sim->stream));
   return LBM_OK;
 }

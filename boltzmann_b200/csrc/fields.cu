@@ -174,6 +174,13 @@ __global__ void narrow_kernel(const double* __restrict__ src, float* __restrict_
     dst[i] = (float)src[i];
 }
 
+// Low four CellFlags bits of the int32 host layout (WALL, FIXED_FLUID_*, FIXED_SCALAR_VALUE).
+__global__ void flags_kernel(const int32_t* __restrict__ src, uint8_t* __restrict__ dst,
+                             int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (uint8_t)(src[i] & 0xF);
+}
+
 __global__ void widen_kernel(const float* __restrict__ src, double* __restrict__ dst, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
@@ -272,6 +279,11 @@ cudaError_t populations_to_aos(const lbm_sim& sim, int tracer, float* d_aos) {
 
 cudaError_t narrow_to_float(const double* src, float* dst, int64_t count, cudaStream_t s) {
   narrow_kernel<<<blocks_for(count), kThreads, 0, s>>>(src, dst, count);
+  return cudaGetLastError();
+}
+
+cudaError_t flags_to_u8(const int32_t* src, uint8_t* dst, int64_t count, cudaStream_t s) {
+  flags_kernel<<<blocks_for(count), kThreads, 0, s>>>(src, dst, count);
   return cudaGetLastError();
 }
 

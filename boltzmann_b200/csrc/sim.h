@@ -65,6 +65,7 @@ cudaError_t populations_from_aos(const lbm_sim& sim, int tracer, const float* d_
 cudaError_t populations_to_aos(const lbm_sim& sim, int tracer, float* d_aos);
 cudaError_t narrow_to_float(const double* src, float* dst, int64_t count, cudaStream_t s);
 cudaError_t widen_to_double(const float* src, double* dst, int64_t count, cudaStream_t s);
+cudaError_t flags_to_u8(const int32_t* src, uint8_t* dst, int64_t count, cudaStream_t s);
 cudaError_t fill_value(void* dst, int64_t count, double value, bool is_double, cudaStream_t s);
 cudaError_t conservation_sums(const lbm_sim& sim, double* d_out);
 
