@@ -50,7 +50,7 @@ def _load() -> dict:
 def _store(entries: dict) -> None:
     p = cache_path()
     p.parent.mkdir(parents=True, exist_ok=True)
-    tmp = p.with_suffix(".tmp")
+    tmp = p.with_suffix(f".{os.getpid()}.tmp")  # ranks of one job may store at the same time
     tmp.write_text(json.dumps(entries, indent=1, sort_keys=True))
     os.replace(tmp, p)
 

@@ -201,6 +201,17 @@ class EnsembleSetup:
             start += a * b
         return out
 
+    def subset(self, indices) -> "EnsembleSetup":
+        """The listed domains only (in the given order), e.g. one rank's shard."""
+        sl = self.domain_slices()
+        pick = lambda a: (np.concatenate([a[sl[i]] for i in indices]) if len(indices)
+                          else a[:0].copy())
+        params = {k: ([v[i] for i in indices] if isinstance(v, list) and len(v) == len(self.counts)
+                      else v) for k, v in self.params.items()}
+        return EnsembleSetup(self.name, [self.counts[i] for i in indices],
+                             [self.tau[i] for i in indices], pick(self.flags), pick(self.rho),
+                             pick(self.vel), params)
+
 
 def lid_driven_cavities(
     count: int = 512,
