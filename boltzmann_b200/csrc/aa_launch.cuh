@@ -2,8 +2,11 @@
 // lattice so the instantiations compile in parallel.
 #pragma once
 
+#include <cudaTypedefs.h>
+
 #include <atomic>
 #include <mutex>
+#include <type_traits>
 
 #include "aa_tma.cuh"
 #include "aa_step.cuh"
@@ -78,6 +81,46 @@ constexpr int tma_stages() {
   return s < 2 ? 2 : (s > 4 ? 4 : s);
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+template <class T>
+constexpr CUtensorMapDataType tensor_map_type() {
+  if constexpr (sizeof(T) == 8) return CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  else if constexpr (sizeof(T) == 4) return CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  else if constexpr (std::is_same_v<T, __half>) return CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+  else return CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+}
+
+// A [q slots][n cells] array (slot stride n elements) as a 2D tensor with a box of
+// kTmaTile cells by all q slots. False when it cannot be described (the caller then copies row
+// segments).
+template <class T>
+bool encode_slot_map(CUtensorMap* map, const void* base, long long n, int q) {
+  auto encode = tensor_map_encoder();
+  if (encode == nullptr || n >= (1ll << 31) || q > 256) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)q};
+  cuuint64_t strides[1] = {(cuuint64_t)n * sizeof(T)};
+  if (strides[0] % 16 != 0 || (reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
+  cuuint32_t box[2] = {(cuuint32_t)kTmaTile, (cuuint32_t)q};
+  cuuint32_t elem[2] = {1, 1};
+  return encode(map, tensor_map_type<T>(), 2, const_cast<void*>(base), dims, strides, box, elem,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <class L, bool TRT, int K, bool EVEN, int NT>
 cudaError_t launch_tma(const StepArgs<typename Pop<K>::real>& a, cudaStream_t stream) {
   constexpr int S = tma_stages<L, K, NT, EVEN>();
@@ -99,7 +142,16 @@ cudaError_t launch_tma(const StepArgs<typename Pop<K>::real>& a, cudaStream_t st
   const long long tiles = (long long)a.nx * a.ny * (a.nz / kTmaTile);
   long long grid = (long long)sms * per_sm;
   if (grid > tiles) grid = tiles;
-  kern<<<(unsigned)grid, kTmaThreads, smem, stream>>>(a);
+  TmaMaps maps{};
+  if constexpr (!EVEN) {
+    using T = typename Pop<K>::type;
+    using Real = typename Pop<K>::real;
+    bool ok = encode_slot_map<T>(&maps.f, a.f, a.n, L::Q);
+    if constexpr (NT == 1)
+      ok = ok && encode_slot_map<Real>(&maps.g, a.tr[0].g, a.n, TracerLattice<L::D>::type::Q);
+    maps.use = ok ? 1 : 0;
+  }
+  kern<<<(unsigned)grid, kTmaThreads, smem, stream>>>(a, maps);
   return cudaGetLastError();
 }
 

@@ -14,7 +14,9 @@
 // bank conflicts), collide, and store straight to HBM with coalesced stores.
 //
 // In-flight data is bounded by shared memory, not by registers, and the copy engine issues one
-// instruction per row segment instead of one per element.
+// instruction per row segment instead of one per element. Odd steps, which read their own row of
+// every slot, take all slots of an array in one tensor-map copy (cp.async.bulk.tensor, a box of
+// 256 cells by Q slots) when the launcher provides the maps.
 //
 // Synchronisation: a producer warp fills stage s once every consumer warp has arrived on the
 // stage's `empty` barrier; consumers wait on its `full` barrier (expected bytes), read their
@@ -24,6 +26,8 @@
 // Every population slot is still read and written by exactly one thread per step, and no tile
 // writes what another tile of the same step reads, so stores need no ordering with the copies.
 #pragma once
+
+#include <cuda.h>
 
 #include <cstdint>
 
@@ -73,6 +77,23 @@ __device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned b
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::
           "r"(smem_u32(dst)),
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Tensor-map copies of the odd step: the population (or tracer) array seen as a [slots][cells]
+// matrix, one {256 cells x all slots} box per tile, landing as [slot][256] in the stage.
+struct TmaMaps {
+  CUtensorMap f;  // populations, box {256, Q}
+  CUtensorMap g;  // fused tracer populations, box {256, Qt}
+  int use;        // 1 when both maps are valid for this launch
+};
+
+__device__ __forceinline__ void tensor_copy_2d(void* dst, const CUtensorMap* map, int c0, int c1,
+                                               uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, "
+      "{%2, %3}], [%4];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
       : "memory");
 }
 
@@ -134,7 +155,8 @@ constexpr int kTmaThreads = kTmaTile + 32;  // + one producer warp
 // barrier (one arrival per consumer warp once it has its operands in registers).
 template <class L, bool TRT, int K, bool EVEN, int NT, int S>
 __global__ void __launch_bounds__(kTmaThreads)
-    aa_tma_kernel(const __grid_constant__ StepArgs<typename Pop<K>::real> a) {
+    aa_tma_kernel(const __grid_constant__ StepArgs<typename Pop<K>::real> a,
+                  const __grid_constant__ TmaMaps maps) {
   using P = Pop<K>;
   using Real = typename P::real;
   using T = typename P::type;
@@ -215,7 +237,7 @@ __global__ void __launch_bounds__(kTmaThreads)
       const int op = lane + 32 * k;
       Job jb{nullptr, 0, 0, 0, 0, 1, 0u, 0};
       if (op < Q) {
-        const int slot = EVEN ? op : opp(op);
+        const int slot = op;  // stage position op holds slot op (odd steps read opp(i) from it)
         const int cz = EVEN && !whole_row ? comp<L>(op, 2) : 0;
         jb.base = reinterpret_cast<const unsigned char*>(static_cast<const T*>(a.f) +
                                                          (size_t)slot * a.n);
@@ -229,7 +251,7 @@ __global__ void __launch_bounds__(kTmaThreads)
       } else if (op < Q + St::NG) {
         if constexpr (NT == 1) {
           const int i = op - Q;
-          const int slot = EVEN ? i : opp(i);
+          const int slot = i;
           const int cz = EVEN && !whole_row ? comp<TL>(i, 2) : 0;
           jb.base = reinterpret_cast<const unsigned char*>(a.tr[0].g + (size_t)slot * a.n);
           jb.cx = EVEN ? comp<TL>(i, 0) : 0;
@@ -272,10 +294,18 @@ __global__ void __launch_bounds__(kTmaThreads)
       const int ym = y == 0 ? a.ny - 1 : y - 1, yp = y == a.ny - 1 ? 0 : y + 1;
       if (lane == 0) mbar_expect_tx(full + s, expect);
       __syncwarp();
+      const bool by_map = !EVEN && maps.use;
+      if (by_map && lane == 0) {
+        // All slots of the tile's cells in one box per array (the row's first cell is a
+        // multiple of 256, so the inner coordinate is 16-byte aligned).
+        const int cell0 = (int)((long long)x * plane + (long long)y * a.nz + z0);
+        tensor_copy_2d(st, &maps.f, cell0, 0, full + s);
+        if constexpr (NT == 1) tensor_copy_2d(st + St::off_trc, &maps.g, cell0, 0, full + s);
+      }
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
         const Job& jb = jobs[k];
-        if (jb.kind == 1) {
+        if (jb.kind == 1 && !by_map) {
           const int ux = jb.cx > 0 ? xm : (jb.cx < 0 ? xp : x);
           const int uy = jb.cy > 0 ? ym : (jb.cy < 0 ? yp : y);
           const unsigned char* row = jb.base + (size_t)(ux * plane + (long long)uy * a.nz) * jb.es;
@@ -312,7 +342,8 @@ __global__ void __launch_bounds__(kTmaThreads)
     Real fv[Q];
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
-      const T* seg = reinterpret_cast<const T*>(st + (size_t)i * St::SEG * sizeof(T));
+      const T* seg =
+          reinterpret_cast<const T*>(st + (size_t)(EVEN ? i : opp(i)) * St::SEG * sizeof(T));
       const int zi = whole_row ? (tid - comp<L>(i, 2)) & (kTmaTile - 1) : tid - comp<L>(i, 2);
       const T v = EVEN ? seg[St::H + zi] : seg[tid];
       if constexpr (dev_in<K>())
@@ -324,8 +355,8 @@ __global__ void __launch_bounds__(kTmaThreads)
     if constexpr (NT == 1) {
 #pragma unroll
       for (int i = 0; i < St::NG; ++i) {
-        const Real* seg =
-            reinterpret_cast<const Real*>(st + St::off_trc + (size_t)i * St::SEGG * sizeof(Real));
+        const Real* seg = reinterpret_cast<const Real*>(
+            st + St::off_trc + (size_t)(EVEN ? i : opp(i)) * St::SEGG * sizeof(Real));
         const int zi = whole_row ? (tid - comp<TL>(i, 2)) & (kTmaTile - 1) : tid - comp<TL>(i, 2);
         g[i] = EVEN ? seg[St::HG + zi] : seg[tid];
       }
