@@ -131,6 +131,22 @@ __device__ __forceinline__ void aa_store(typename P::type* __restrict__ f, long 
   }
 }
 
+// Where update_cell puts the post-collision populations: the AA store straight to HBM. (The
+// TMA kernel passes a sink that writes them into its shared-memory stage instead, from where whole
+// row segments go back with bulk copies.)
+struct GlobalSink {
+  template <class L, class P, bool EVEN, bool DEV>
+  __device__ __forceinline__ void fluid(typename P::type* f, long long n, const CellPos& c,
+                                        const typename P::real (&v)[L::Q]) const {
+    aa_store<L, P, EVEN, DEV>(f, n, c, v);
+  }
+  template <class TL, class TP, bool EVEN>
+  __device__ __forceinline__ void tracer(typename TP::type* g, long long n, const CellPos& c,
+                                         const typename TP::real (&v)[TL::Q]) const {
+    aa_store<TL, TP, EVEN, false>(g, n, c, v);
+  }
+};
+
 // BGK or TRT collision against the second-order equilibrium
 //   feq_i = w_i r (1 + 3 c_i.u + 4.5 (c_i.u)^2 - 1.5 u.u),
 // evaluated per opposite pair (i, i+1) as feq = A +- B (symmetric and antisymmetric parts).
@@ -334,10 +350,11 @@ __device__ __forceinline__ void moments_packed(float (&v)[L::Q], float& dr, floa
 
 // Advection-diffusion update of one tracer cell in the fluid velocity u just computed
 // (src/lib.cl:102-189, 303-405), with its populations already loaded into g.
-template <class TL, class TP, bool EVEN, class Real>
+template <class TL, class TP, bool EVEN, class Real, class Sink = GlobalSink>
 __device__ __forceinline__ void tracer_update(const TracerArgs<Real>& tr, long long n,
                                               const CellPos& c, int flag, Real (&g)[TL::Q],
-                                              const Real (&u)[3], Real uu, bool keep) {
+                                              const Real (&u)[3], Real uu, bool keep,
+                                              const Sink& sink = Sink()) {
   Real rt = 0;
 #pragma unroll
   for (int i = 0; i < TL::Q; ++i) rt += g[i];
@@ -351,7 +368,7 @@ __device__ __forceinline__ void tracer_update(const TracerArgs<Real>& tr, long l
     collide_packed<TL, false, false>(g, rt, rt, u, uu, om, om);
   else
     collide<TL, false, false>(g, rt, rt, u, uu, om, om);
-  aa_store<TL, TP, EVEN, false>(tr.g, n, c, g);
+  sink.template tracer<TL, TP, EVEN>(tr.g, n, c, g);
   if (keep && !tfixed) tr.val[c.cell] = rt;
 }
 
@@ -381,14 +398,15 @@ __device__ __forceinline__ CellPos make_cellpos(const StepArgs<Real>& a, int x, 
 // (NT == 1), cval the coupled tracer's previous value.
 // om_pos / om_neg are the relaxation rates of the cell's domain (a.om_pos / a.om_neg for a single
 // simulation; per domain in an ensemble).
-template <class L, bool TRT, int K, bool EVEN, int NT>
+template <class L, bool TRT, int K, bool EVEN, int NT, class Sink = GlobalSink>
 __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real>& a,
                                             const CellPos& c, int flag,
                                             typename Pop<K>::real (&f)[L::Q],
                                             typename Pop<K>::real (&g)[NT == 1 ? TracerLattice<L::D>::type::Q : 1],
                                             typename Pop<K>::real cval,
                                             typename Pop<K>::real om_pos,
-                                            typename Pop<K>::real om_neg) {
+                                            typename Pop<K>::real om_neg,
+                                            const Sink& sink = Sink()) {
   using P = Pop<K>;
   using Real = typename P::real;
   using T = typename P::type;
@@ -464,7 +482,7 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
     collide_packed<L, TRT, true>(f, r, dr, u, uu, om_pos, om_neg);
   else
     collide<L, TRT, true>(f, r, dr, u, uu, om_pos, om_neg);
-  aa_store<L, P, EVEN, true>(static_cast<T*>(a.f), a.n, c, f);
+  sink.template fluid<L, P, EVEN, true>(static_cast<T*>(a.f), a.n, c, f);
 
   if (a.write_moments && !fixed) {
     a.rho[c.cell] = r;
@@ -475,7 +493,7 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
 
   if constexpr (NT == 1) {
     const bool keep = a.write_moments || (a.acc_mode == kAccBoussinesq && a.coupled == 0);
-    tracer_update<TL, TP, EVEN>(a.tr[0], a.n, c, flag, g, u, uu, keep);
+    tracer_update<TL, TP, EVEN>(a.tr[0], a.n, c, flag, g, u, uu, keep, sink);
   } else if constexpr (NT < 0) {
     for (int t = 0; t < a.ntracers; ++t) {
       Real gt[TL::Q];
