@@ -177,8 +177,9 @@ __global__ void narrow_kernel(const double* __restrict__ src, float* __restrict_
 // Low four CellFlags bits of the int32 host layout (WALL, FIXED_FLUID_*, FIXED_SCALAR_VALUE).
 __global__ void flags_kernel(const int32_t* __restrict__ src, uint8_t* __restrict__ dst,
                              int64_t n) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < n) dst[i] = (uint8_t)(src[i] & 0xF);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = (uint8_t)(src[i] & 0xF);
 }
 
 __global__ void widen_kernel(const float* __restrict__ src, double* __restrict__ dst, int64_t n) {

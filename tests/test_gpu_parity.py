@@ -197,6 +197,30 @@ def test_cylinder_channel_small():
     assert rel_err(gpu.vals[0], ref.tracers["tracer"].val) < PARITY
 
 
+def test_cylinder_channel_full_size_flags_and_two_steps():
+    """The channel at its full 4096x2048 size (8.4M cells, more than one grid's worth of the
+    set-up kernels): every wall keeps its density and every fixed column its velocity, however
+    far into the array it lies, and one AA step pair matches the oracle."""
+    from boltzmann_b200 import workloads
+
+    setup = workloads.cylinder_channel()
+    assert int(np.prod(setup.counts)) > 148 * 64 * 256
+    gpu = _capi_like(setup)
+    flags, rho0, vel0 = gpu.flags.copy(), gpu.rho.copy(), gpu.vel.copy()
+    gpu.iterate(2)
+    wall = (flags & 1) == 1
+    fixed = ((flags & 6) != 0) & ~wall
+    assert wall[-1].any() and fixed[-1].any()
+    np.testing.assert_array_equal(gpu.rho[wall], rho0[wall])
+    np.testing.assert_array_equal(gpu.vel[fixed], vel0[fixed])
+    backend = "reference" if reference_available() else "port"
+    ref = _oracle_like(setup, backend)
+    ref.iterate(2)
+    assert rel_err(gpu.rho, ref.rho) < PARITY
+    assert rel_err(gpu.vel, ref.vel) < PARITY
+    assert rel_err(gpu.vals[0], ref.tracers["tracer"].val) < PARITY
+
+
 def test_odd_iters_and_missing_kernels():
     from tests.capi import CApiSim
 
