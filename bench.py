@@ -403,7 +403,7 @@ def cpu_ensemble_rate(setup, budget_s: float) -> dict:
 
 
 def run_ensemble(args) -> None:
-    """512 lid-driven cavities advanced in one persistent launch per step,
+    """The cavity ensemble: 512 lid-driven cavities advanced in one persistent launch per step,
     replayed from a CUDA graph, autotuned tile shape; per-domain launches timed for comparison."""
     import torch
 

@@ -121,11 +121,11 @@ bool encode_slot_map(CUtensorMap* map, const void* base, long long n, int q) {
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <class L, bool TRT, int K, bool EVEN, int NT>
+template <class L, bool TRT, int K, bool EVEN, int NT, bool WR>
 cudaError_t launch_tma(const StepArgs<typename Pop<K>::real>& a, cudaStream_t stream) {
   constexpr int S = tma_stages<L, K, NT, EVEN>();
   constexpr size_t smem = tma_smem_bytes<L, K, NT, EVEN, S>();
-  auto kern = aa_tma_kernel<L, TRT, K, EVEN, NT, S>;
+  auto kern = aa_tma_kernel<L, TRT, K, EVEN, NT, S, WR>;
   static std::once_flag once;
   static cudaError_t setup_err = cudaSuccess;
   static int per_sm = 1;
@@ -165,7 +165,11 @@ cudaError_t launch_one(const StepArgs<typename Pop<K>::real>& a, cudaStream_t st
     const long long tiles = (long long)a.nx * a.ny * (a.nz / kTmaTile);
     const bool fits = a.nz % kTmaTile == 0;
     const bool staged = a.path == 2 || (a.path == 0 && tiles >= 8LL * 148);
-    if (fits && staged) return launch_tma<L, TRT, K, EVEN, NT>(a, stream);
+    if (fits && staged) {
+      if constexpr (EVEN)
+        if (a.nz == kTmaTile) return launch_tma<L, TRT, K, EVEN, NT, true>(a, stream);
+      return launch_tma<L, TRT, K, EVEN, NT, false>(a, stream);
+    }
   }
   dim3 grid, block;
   step_geometry(a, grid, block);

@@ -11,18 +11,22 @@
 // when a row is a single tile the plain row is copied and the index wraps in shared memory) --
 // plus the fused tracer's populations, the coupled tracer value and the flag bytes.
 // Threads read their operands from shared memory (consecutive threads, consecutive words: no
-// bank conflicts), collide, and store straight to HBM with coalesced stores.
+// bank conflicts) and collide. Odd steps, and even steps whose rows are one tile, write their
+// results back into the stage slot they came from, and the producer warp writes the stage back
+// with one bulk store per row segment (cp.async.bulk shared -> global) before refilling it.
+// Other even steps store straight to HBM with coalesced stores.
 //
 // In-flight data is bounded by shared memory, not by registers, and the copy engine issues one
 // instruction per row segment instead of one per element. Odd steps, which read their own row of
 // every slot, take all slots of an array in one tensor-map copy (cp.async.bulk.tensor, a box of
 // 256 cells by Q slots) when the launcher provides the maps.
 //
-// Synchronisation: a producer warp fills stage s once every consumer warp has arrived on the
-// stage's `empty` barrier; consumers wait on its `full` barrier (expected bytes), read their
-// operands into registers, arrive on `empty`, then compute and store. There is no CTA-wide
-// barrier in the loop. Every wait is bounded: on timeout the kernel sets bit 1 (value 2) of the
-// status word and leaves.
+// Synchronisation: stage s has a `full` mbarrier (the producer's expect_tx plus the copies'
+// bytes) and an `empty` one (one arrival per consumer warp: once its operands are in registers,
+// or, when results go back through the stage, once they are written there). Before refilling
+// stage s the producer waits on `empty`, issues the stage's bulk stores if it holds results and
+// waits until they have read it. There is no CTA-wide barrier in the loop. Every wait is
+// bounded: on timeout the kernel sets bit 1 (value 2) of the status word and leaves.
 // Every population slot is still read and written by exactly one thread per step, and no tile
 // writes what another tile of the same step reads, so stores need no ordering with the copies.
 #pragma once
@@ -119,22 +123,6 @@ __device__ __forceinline__ void bulk_wait_all() {
   asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
 }
 
-// Named barrier 1 over the 256 consumer threads (the producer warp never takes part).
-__device__ __forceinline__ void consumers_sync() {
-  asm volatile("bar.sync 1, 256;\n" ::: "memory");
-}
-// The same barrier, returning whether `ok` held in every consumer thread.
-__device__ __forceinline__ bool consumers_all(bool ok) {
-  unsigned r;
-  asm volatile(
-      "{\n .reg .pred q, p;\n setp.ne.u32 q, %1, 0;\n bar.red.and.pred p, 1, 256, q;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(r)
-      : "r"(ok ? 1u : 0u)
-      : "memory");
-  return r != 0;
-}
-
 // Shared-memory layout of one stage, in elements of each operand's type.
 template <class L, int K, int NT, bool EVEN>
 struct TmaStage {
@@ -222,10 +210,8 @@ struct StageSink {
 constexpr int kConsumerWarps = kTmaTile / 32;
 constexpr int kTmaThreads = kTmaTile + 32;  // + one producer warp
 
-// Warp-specialised: warps 0..7 consume (one cell per thread), warp 8 produces. Stage s has a
-// `full` barrier (one arrival: the producer's expect_tx, plus the copies' bytes) and an `empty`
-// barrier (one arrival per consumer warp once it has its operands in registers).
-template <class L, bool TRT, int K, bool EVEN, int NT, int S>
+// Warp-specialised: warps 0..7 consume (one cell per thread), warp 8 loads and stores stages.
+template <class L, bool TRT, int K, bool EVEN, int NT, int S, bool WR>
 __global__ void __launch_bounds__(kTmaThreads)
     aa_tma_kernel(const __grid_constant__ StepArgs<typename Pop<K>::real> a,
                   const __grid_constant__ TmaMaps maps) {
@@ -277,16 +263,19 @@ __global__ void __launch_bounds__(kTmaThreads)
     }
   };
 
-  // Odd steps write their populations back through the stage (bulk stores of the tile's own row
-  // segments, one arrival on `empty` once they have read it); even steps store from registers
-  // and release the stage warp by warp as soon as the operands are read. (Bulk stores on even
-  // steps of one-tile rows were correct but measured 15% slower with FP16 populations: the stage
-  // stays busy through the collision, and the ring runs dry.)
-  const bool bulk_out = !EVEN;
+  // WR: every row is one tile (nz == T; even steps only). Odd steps, and even steps of one-tile
+  // rows, leave their results in the stage, and the producer writes the stage back as whole row
+  // segments before refilling it (bulk stores). Other even steps store from registers (their
+  // results' segments are shifted by c_iz, so not 16-byte aligned) and release the stage warp by
+  // warp as soon as the operands are read. (Bulk stores of the aligned part with plain stores
+  // of the two partial chunks per slot were correct there but made the producer the limit:
+  // -8% with FP32, -17% with FP16 populations on the 4096x2048 channel.)
+  constexpr bool whole_row = WR;
+  constexpr bool bulk_out = !EVEN || WR;
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(full + s, 1);
-      mbar_init(empty + s, bulk_out ? 1 : kConsumerWarps);
+      mbar_init(empty + s, kConsumerWarps);
     }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -307,7 +296,6 @@ __global__ void __launch_bounds__(kTmaThreads)
       unsigned dst;               // byte offset inside a stage of element z0 - hl
       int kind;                   // 0 none, 1 row segment with halo, 2 own tile (no halo)
     };
-    const bool whole_row = a.nz == kTmaTile;
     Job jobs[2];
     unsigned lane_bytes = 0;
 #pragma unroll
@@ -358,6 +346,34 @@ __global__ void __launch_bounds__(kTmaThreads)
     }
     const unsigned expect = __reduce_add_sync(0xffffffffu, lane_bytes);
     const long long plane = (long long)a.ny * a.nz;
+    // First byte of the row a job's segment of tile (x, y) comes from: the tile's own row, or
+    // the row upstream of the job's direction on even steps.
+    auto job_row = [&](const Job& jb, int x, int y) {
+      const int ux = jb.cx > 0 ? (x == 0 ? a.nx - 1 : x - 1) : (jb.cx < 0 ? (x == a.nx - 1 ? 0 : x + 1) : x);
+      const int uy = jb.cy > 0 ? (y == 0 ? a.ny - 1 : y - 1) : (jb.cy < 0 ? (y == a.ny - 1 ? 0 : y + 1) : y);
+      return jb.base + (size_t)(ux * plane + (long long)uy * a.nz) * jb.es;
+    };
+    // With bulk_out the consumers leave a tile's results in its stage: each population and
+    // tracer segment goes back to the row it came from (no halo then: odd steps read their own
+    // row, even steps of one-tile rows the whole row), and the stage is refilled once the
+    // stores have read it.
+    TileWalker tws;
+    tws.init(blockIdx.x, gridDim.x, a.ny, tiles_per_row);
+    auto store_stage = [&](int s) {
+      const unsigned char* st = stage_ptr(s);
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const Job& jb = jobs[k];
+        if (jb.kind == 1)
+          bulk_store(const_cast<unsigned char*>(job_row(jb, tws.x, tws.y)) +
+                         (size_t)tws.zt * kTmaTile * jb.es,
+                     st + jb.dst, (unsigned)(kTmaTile * jb.es));
+      }
+      bulk_commit();
+      bulk_wait_read();
+      __syncwarp();
+      tws.next();
+    };
     bool ok = true;
     int produced = 0;
     TileWalker tw;
@@ -366,10 +382,9 @@ __global__ void __launch_bounds__(kTmaThreads)
       const int s = j % S;
       if (j >= S) ok = mbar_wait(empty + s, (unsigned)(((j / S) - 1) & 1));
       if (!__all_sync(0xffffffffu, ok)) break;
+      if (j >= S && bulk_out) store_stage(s);
       const int x = tw.x, y = tw.y, z0 = tw.zt * kTmaTile;
       unsigned char* st = stage_ptr(s);
-      const int xm = x == 0 ? a.nx - 1 : x - 1, xp = x == a.nx - 1 ? 0 : x + 1;
-      const int ym = y == 0 ? a.ny - 1 : y - 1, yp = y == a.ny - 1 ? 0 : y + 1;
       if (lane == 0) mbar_expect_tx(full + s, expect);
       __syncwarp();
       const bool by_map = !EVEN && maps.use;
@@ -384,10 +399,8 @@ __global__ void __launch_bounds__(kTmaThreads)
       for (int k = 0; k < 2; ++k) {
         const Job& jb = jobs[k];
         if (jb.kind == 1 && !by_map) {
-          const int ux = jb.cx > 0 ? xm : (jb.cx < 0 ? xp : x);
-          const int uy = jb.cy > 0 ? ym : (jb.cy < 0 ? yp : y);
-          const unsigned char* row = jb.base + (size_t)(ux * plane + (long long)uy * a.nz) * jb.es;
-          copy_row_segment(st + jb.dst, row, z0, jb.hl, jb.hr, a.nz, jb.es, full + s);
+          copy_row_segment(st + jb.dst, job_row(jb, x, y), z0, jb.hl, jb.hr, a.nz, jb.es,
+                           full + s);
         } else if (jb.kind == 2) {
           const long long first = (long long)x * plane + (long long)y * a.nz + z0;
           bulk_copy(st + jb.dst, jb.base + (size_t)first * jb.es, (unsigned)(kTmaTile * jb.es),
@@ -396,6 +409,14 @@ __global__ void __launch_bounds__(kTmaThreads)
       }
       produced = j + 1;
     }
+    // The last tiles' results (bounded waits for the consumers), then every store complete.
+    if (bulk_out && ok) {
+      for (int j = produced - S > 0 ? produced - S : 0; j < produced && ok; ++j) {
+        ok = __all_sync(0xffffffffu, mbar_wait(empty + j % S, (unsigned)((j / S) & 1)));
+        if (ok) store_stage(j % S);
+      }
+    }
+    if (bulk_out) bulk_wait_all();
     if (!ok && lane == 0) atomicOr(a.status, 2);
     // Leave only once the copies of the last stages have landed (bounded), so that no copy
     // writes into shared memory after the CTA is gone.
@@ -406,15 +427,13 @@ __global__ void __launch_bounds__(kTmaThreads)
   }
 
   // ---- consumer warps: thread tid owns cell z0 + tid of every tile.
-  const bool whole_row = a.nz == kTmaTile;
   TileWalker tw;
   tw.init(blockIdx.x, gridDim.x, a.ny, tiles_per_row);
   for (int j = 0; j < count; ++j, tw.next()) {
     const int s = j % S;
-    bool ok = mbar_wait(full + s, (unsigned)((j / S) & 1));
-    if (bulk_out) ok = consumers_all(ok);  // the consumers stay in step: they share barrier 1
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(full + s, (unsigned)((j / S) & 1)));
     if (!ok) {
-      atomicOr(a.status, 2);
+      if (lane == 0) atomicOr(a.status, 2);
       break;  // the producer's own waits are bounded too
     }
     const int x = tw.x, y = tw.y, z0 = tw.zt * kTmaTile;
@@ -452,42 +471,13 @@ __global__ void __launch_bounds__(kTmaThreads)
       update_cell<L, TRT, K, EVEN, NT>(a, c, flag, fv, g, cval, a.om_pos, a.om_neg);
       continue;
     }
+    // Results into the stage, where the producer picks them up as whole row segments.
     const StageSink<St, L, TL> sink{const_cast<unsigned char*>(st), tid};
     update_cell<L, TRT, K, EVEN, NT>(a, c, flag, fv, g, cval, a.om_pos, a.om_neg, sink);
     fence_proxy_async();  // this thread's stage writes, visible to the bulk stores
-    consumers_sync();
-    if (warp == 0) {
-      // Lane k stores slot k (and k + 32): the tile's row segment of the thread's own row (odd
-      // steps) or the whole upstream row (even steps of one-tile rows).
-      const long long plane = (long long)a.ny * a.nz;
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const int op = lane + 32 * k;
-        if (op < Q) {
-          const int ux = EVEN ? (x - comp<L>(op, 0) + a.nx) % a.nx : x;
-          const int uy = EVEN ? (y - comp<L>(op, 1) + a.ny) % a.ny : y;
-          T* dst = static_cast<T*>(a.f) + (size_t)op * a.n + (size_t)(ux * plane) +
-                   (size_t)uy * a.nz + z0;
-          bulk_store(dst, st + ((size_t)op * St::SEG + St::H) * sizeof(T),
-                     (unsigned)(kTmaTile * sizeof(T)));
-        } else if (op < Q + St::NG) {
-          if constexpr (NT == 1) {
-            const int i = op - Q;
-            const int ux = EVEN ? (x - comp<TL>(i, 0) + a.nx) % a.nx : x;
-            const int uy = EVEN ? (y - comp<TL>(i, 1) + a.ny) % a.ny : y;
-            Real* dst = a.tr[0].g + (size_t)i * a.n + (size_t)(ux * plane) + (size_t)uy * a.nz + z0;
-            bulk_store(dst, st + St::off_trc + ((size_t)i * St::SEGG + St::HG) * sizeof(Real),
-                       (unsigned)(kTmaTile * sizeof(Real)));
-          }
-        }
-      }
-      bulk_commit();
-      bulk_wait_read();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(empty + s);  // the stage's contents have been read out
-    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(empty + s);
   }
-  if (bulk_out && warp == 0) bulk_wait_all();  // the tile stores are complete before exit
 }
 
 }  // namespace lbm

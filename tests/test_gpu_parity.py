@@ -3,7 +3,7 @@ oracle.
 
 Tolerances (norm-wise relative, ||gpu - ref|| / ||ref||): the CUDA kernels collide in FP32 while
 the reference evaluates its double literals in double, so results differ by rounding only:
-  - PARITY = 1e-5 for rho, vel, tracer values and populations (the north-star bound);
+  - PARITY = 1e-5 for rho, vel, tracer values and populations (the FP32 parity bound);
   - equilibrium initialisation is bit-exact (same FP32 operation order as the reference).
 """
 
@@ -152,7 +152,7 @@ def _capi_like(setup, storage="f32"):
 
 
 def test_kelvin_helmholtz_1000_steps():
-    """BASELINE config 1 at full size: D2Q9 BGK 256^2, tau 0.55, 1000 steps."""
+    """The Kelvin-Helmholtz shear layer at full size: D2Q9 BGK 256^2, tau 0.55, 1000 steps."""
     from boltzmann_b200 import workloads
 
     setup = workloads.kelvin_helmholtz()
@@ -182,7 +182,7 @@ def test_taylor_green_d3q27(collision):
 
 
 def test_cylinder_channel_small():
-    """BASELINE config 2 scaled to 512x256 (radius 8): TRT + walls + fixed columns + tracer +
+    """The cylinder channel scaled to 512x256 (radius 8): TRT + walls + fixed columns + tracer +
     Boussinesq, 200 steps."""
     from boltzmann_b200 import workloads
 
@@ -326,6 +326,10 @@ TMA_CASES = {
                                      tracers=[["t0", ["bgk", 0.6]]],
                                      couplings=[["t0", 0.1, 0.5, [0.0, -0.01]]], calls=[4, 6]),
     "d2q9_single_row": dict(counts=[1, 256], omega=["bgk", 0.7], calls=[4]),
+    "d2q9_trt_tracer_one_tile_rows": dict(counts=[24, 256], omega=["trt", 0.57], walls=True,
+                                          tracers=[["t0", ["bgk", 0.62]]],
+                                          couplings=[["t0", 0.1, 0.5, [0.0, -0.01]]],
+                                          calls=[2, 4]),
     "d3q27_bgk_walls_gravity": dict(counts=[5, 4, 256], omega=["bgk", 0.55], walls=True,
                                     gravity=[1e-3, 0.0, -1e-3], calls=[4]),
     "d3q27_trt_tracer_coupling": dict(counts=[3, 3, 256], omega=["trt", 0.58], walls=True,
