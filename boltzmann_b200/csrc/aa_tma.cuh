@@ -101,6 +101,17 @@ __device__ __forceinline__ void tensor_copy_2d(void* dst, const CUtensorMap* map
       : "memory");
 }
 
+// The reverse: one box from shared memory back to the tensor (completion tracked by the bulk
+// group, like bulk_store). The coordinates are non-negative and the inner one a multiple of 256.
+__device__ __forceinline__ void tensor_store_2d(const CUtensorMap* map, int c0, int c1,
+                                                const void* src) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"(
+          reinterpret_cast<uint64_t>(map)),
+      "r"(c0), "r"(c1), "r"(smem_u32(src))
+      : "memory");
+}
+
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
 }
@@ -210,9 +221,19 @@ struct StageSink {
 constexpr int kConsumerWarps = kTmaTile / 32;
 constexpr int kTmaThreads = kTmaTile + 32;  // + one producer warp
 
+// CTAs per SM the register allocation is asked to allow. 32- and 64-bit populations: one, so
+// the compiler keeps more of each cell in registers (~90 for FP32 D3Q27, ~80 for the fused
+// D2Q9 + tracer even step) and two CTAs share an SM; measured 3-5% faster than three leaner CTAs.
+// 16-bit populations move half the bytes and need the occupancy instead: three CTAs for D3Q27,
+// four for D2Q9 (one CTA a SM cost them 15%).
+template <class L, int K>
+constexpr int tma_min_blocks() {
+  return (K == kF16 || K == kBF16) ? (L::Q >= 27 ? 3 : 4) : 1;
+}
+
 // Warp-specialised: warps 0..7 consume (one cell per thread), warp 8 loads and stores stages.
 template <class L, bool TRT, int K, bool EVEN, int NT, int S, bool WR>
-__global__ void __launch_bounds__(kTmaThreads)
+__global__ void __launch_bounds__(kTmaThreads, tma_min_blocks<L, K>())
     aa_tma_kernel(const __grid_constant__ StepArgs<typename Pop<K>::real> a,
                   const __grid_constant__ TmaMaps maps) {
   using P = Pop<K>;
@@ -361,13 +382,23 @@ __global__ void __launch_bounds__(kTmaThreads)
     tws.init(blockIdx.x, gridDim.x, a.ny, tiles_per_row);
     auto store_stage = [&](int s) {
       const unsigned char* st = stage_ptr(s);
+      if (!EVEN && maps.use) {
+        // Odd steps: the tile's own row of every slot, the box the tensor-map load brought in.
+        if (lane == 0) {
+          const int cell0 = (int)((long long)tws.x * plane + (long long)tws.y * a.nz +
+                                  (long long)tws.zt * kTmaTile);
+          tensor_store_2d(&maps.f, cell0, 0, st);
+          if constexpr (NT == 1) tensor_store_2d(&maps.g, cell0, 0, st + St::off_trc);
+        }
+      } else {
 #pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const Job& jb = jobs[k];
-        if (jb.kind == 1)
-          bulk_store(const_cast<unsigned char*>(job_row(jb, tws.x, tws.y)) +
-                         (size_t)tws.zt * kTmaTile * jb.es,
-                     st + jb.dst, (unsigned)(kTmaTile * jb.es));
+        for (int k = 0; k < 2; ++k) {
+          const Job& jb = jobs[k];
+          if (jb.kind == 1)
+            bulk_store(const_cast<unsigned char*>(job_row(jb, tws.x, tws.y)) +
+                           (size_t)tws.zt * kTmaTile * jb.es,
+                       st + jb.dst, (unsigned)(kTmaTile * jb.es));
+        }
       }
       bulk_commit();
       bulk_wait_read();
