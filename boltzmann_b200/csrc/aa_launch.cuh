@@ -74,9 +74,9 @@ void step_geometry(const StepArgs<Real>& a, dim3& grid, dim3& block) {
 // Ring depth of the TMA kernel: as many stages as fit in ~50 KB per CTA (2-4), so that three or
 // four CTAs (24-32 consumer warps) share an SM and each keeps one or more tiles of copies in
 // flight while it computes another.
-template <class L, int K, int NT, bool EVEN>
+template <class L, int K, int NT, bool EVEN, bool WR>
 constexpr int tma_stages() {
-  constexpr size_t b = TmaStage<L, K, NT, EVEN>::bytes;
+  constexpr size_t b = TmaStage<L, K, NT, EVEN, WR>::bytes;
   constexpr int s = (int)((50 * 1024) / b);
   return s < 2 ? 2 : (s > 4 ? 4 : s);
 }
@@ -121,10 +121,27 @@ bool encode_slot_map(CUtensorMap* map, const void* base, long long n, int q) {
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// The population array as a 2D tensor of rows of nz cells, row (slot, x, y), with a box of one
+// row of kTmaTile cells (the four-row copies of even steps of one-tile rows).
+template <class T>
+bool encode_row_map(CUtensorMap* map, const void* base, long long rows, int nz) {
+  auto encode = tensor_map_encoder();
+  if (encode == nullptr || rows >= (1ll << 31) || nz != kTmaTile) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)nz, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)nz * sizeof(T)};
+  if (strides[0] % 16 != 0 || (reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
+  cuuint32_t box[2] = {(cuuint32_t)kTmaTile, 1};
+  cuuint32_t elem[2] = {1, 1};
+  return encode(map, tensor_map_type<T>(), 2, const_cast<void*>(base), dims, strides, box, elem,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <class L, bool TRT, int K, bool EVEN, int NT, bool WR>
 cudaError_t launch_tma(const StepArgs<typename Pop<K>::real>& a, cudaStream_t stream) {
-  constexpr int S = tma_stages<L, K, NT, EVEN>();
-  constexpr size_t smem = tma_smem_bytes<L, K, NT, EVEN, S>();
+  constexpr int S = tma_stages<L, K, NT, EVEN, WR>();
+  constexpr size_t smem = tma_smem_bytes<L, K, NT, EVEN, S, WR>();
   auto kern = aa_tma_kernel<L, TRT, K, EVEN, NT, S, WR>;
   static std::once_flag once;
   static cudaError_t setup_err = cudaSuccess;
@@ -143,7 +160,10 @@ cudaError_t launch_tma(const StepArgs<typename Pop<K>::real>& a, cudaStream_t st
   long long grid = (long long)sms * per_sm;
   if (grid > tiles) grid = tiles;
   TmaMaps maps{};
-  if constexpr (!EVEN) {
+  if constexpr (EVEN && WR) {
+    using T = typename Pop<K>::type;
+    maps.use = encode_row_map<T>(&maps.f, a.f, (long long)L::Q * a.nx * a.ny, a.nz) ? 1 : 0;
+  } else if constexpr (!EVEN) {
     using T = typename Pop<K>::type;
     using Real = typename Pop<K>::real;
     bool ok = encode_slot_map<T>(&maps.f, a.f, a.n, L::Q);

@@ -87,9 +87,10 @@ __device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned b
 // Tensor-map copies of the odd step: the population (or tracer) array seen as a [slots][cells]
 // matrix, one {256 cells x all slots} box per tile, landing as [slot][256] in the stage.
 struct TmaMaps {
-  CUtensorMap f;  // populations, box {256, Q}
-  CUtensorMap g;  // fused tracer populations, box {256, Qt}
-  int use;        // 1 when both maps are valid for this launch
+  CUtensorMap f;  // odd steps: populations, box {256, Q}; even steps of one-tile rows: the
+                  // population array as rows of 256 cells, row (slot, x, y), box {256, 1}
+  CUtensorMap g;  // odd steps: fused tracer populations, box {256, Qt}
+  int use;        // 1 when the maps this launch needs are valid
 };
 
 __device__ __forceinline__ void tensor_copy_2d(void* dst, const CUtensorMap* map, int c0, int c1,
@@ -109,6 +110,26 @@ __device__ __forceinline__ void tensor_store_2d(const CUtensorMap* map, int c0, 
       "cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"(
           reinterpret_cast<uint64_t>(map)),
       "r"(c0), "r"(c1), "r"(smem_u32(src))
+      : "memory");
+}
+
+// Four rows of a 2D tensor (x from 0, rows r0..r3; a box one row high) into four consecutive
+// rows of shared memory, and the reverse.
+__device__ __forceinline__ void tensor_gather4(void* dst, const CUtensorMap* map, int r0, int r1,
+                                               int r2, int r3, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(r0), "r"(r1), "r"(r2), "r"(r3),
+      "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tensor_scatter4(const CUtensorMap* map, int r0, int r1, int r2,
+                                                int r3, const void* src) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.global.shared::cta.tile::scatter4.bulk_group "
+      "[%0, {%1, %2, %3, %4, %5}], [%6];\n" ::"l"(reinterpret_cast<uint64_t>(map)),
+      "r"(0), "r"(r0), "r"(r1), "r"(r2), "r"(r3), "r"(smem_u32(src))
       : "memory");
 }
 
@@ -135,31 +156,33 @@ __device__ __forceinline__ void bulk_wait_all() {
 }
 
 // Shared-memory layout of one stage, in elements of each operand's type.
-template <class L, int K, int NT, bool EVEN>
+// WR: rows of one tile (even steps then copy whole rows and need no halo).
+template <class L, int K, int NT, bool EVEN, bool WR = false>
 struct TmaStage {
   using T = typename Pop<K>::type;
   using Real = typename Pop<K>::real;
   using TL = typename TracerLattice<L::D>::type;
   static constexpr int Q = L::Q;
   static constexpr int NG = NT == 1 ? TL::Q : 0;
-  static constexpr int H = EVEN ? 16 / (int)sizeof(T) : 0;       // population halo
-  static constexpr int HG = EVEN ? 16 / (int)sizeof(Real) : 0;   // tracer halo
+  static constexpr int H = EVEN && !WR ? 16 / (int)sizeof(T) : 0;      // population halo
+  static constexpr int HG = EVEN && !WR ? 16 / (int)sizeof(Real) : 0;  // tracer halo
   static constexpr int SEG = kTmaTile + 2 * H;                   // populations per direction
   static constexpr int SEGG = kTmaTile + 2 * HG;
   static constexpr size_t pop_bytes = (size_t)Q * SEG * sizeof(T);
   static constexpr size_t trc_bytes = (size_t)NG * SEGG * sizeof(Real);
   static constexpr size_t val_bytes = (size_t)kTmaTile * sizeof(Real);
   static constexpr size_t flag_bytes = kTmaTile;
-  // offsets (bytes) inside a stage; every part 16-byte aligned
+  // offsets (bytes) inside a stage; every part 16-byte aligned, stages 128-byte aligned (the
+  // tensor copies' shared-memory boxes start on 128 bytes)
   static constexpr size_t off_trc = pop_bytes;
   static constexpr size_t off_val = off_trc + trc_bytes;
   static constexpr size_t off_flag = off_val + val_bytes;
-  static constexpr size_t bytes = off_flag + flag_bytes;
+  static constexpr size_t bytes = (off_flag + flag_bytes + 127) / 128 * 128;
 };
 
-template <class L, int K, int NT, bool EVEN, int S>
+template <class L, int K, int NT, bool EVEN, int S, bool WR = false>
 __host__ __device__ constexpr size_t tma_smem_bytes() {
-  return (size_t)S * TmaStage<L, K, NT, EVEN>::bytes + 16 * S;  // + full/empty mbarriers
+  return (size_t)S * TmaStage<L, K, NT, EVEN, WR>::bytes + 16 * S;  // + full/empty mbarriers
 }
 
 // Bulk-copies the row segment [z0 - hl, z0 + T + hr) of one operand row (elements of `es` bytes)
@@ -240,7 +263,7 @@ __global__ void __launch_bounds__(kTmaThreads, tma_min_blocks<L, K>())
   using Real = typename P::real;
   using T = typename P::type;
   using TL = typename TracerLattice<L::D>::type;
-  using St = TmaStage<L, K, NT, EVEN>;
+  using St = TmaStage<L, K, NT, EVEN, WR>;
   constexpr int Q = L::Q;
   constexpr int NOPS = Q + St::NG + 2;  // copy jobs per tile: populations, tracer, value, flags
 
@@ -316,13 +339,20 @@ __global__ void __launch_bounds__(kTmaThreads, tma_min_blocks<L, K>())
       int hl, hr, es;             // left / right halo (elements), element size (bytes)
       unsigned dst;               // byte offset inside a stage of element z0 - hl
       int kind;                   // 0 none, 1 row segment with halo, 2 own tile (no halo)
+      bool gathered;              // moved by the four-row tensor copies instead (see below)
     };
+    // Even steps of one-tile rows: slots 0 .. 4 NG4 - 1 travel four rows at a time
+    // (tile::gather4 / scatter4 over the population array seen as rows of 256 cells, row
+    // (slot, x, y)); lane k < NG4 moves slots 4k .. 4k + 3. The remaining slots keep their own
+    // copies.
+    constexpr int NG4 = EVEN && WR ? Q / 4 : 0;
+    const bool by_rows = NG4 > 0 && maps.use;
     Job jobs[2];
     unsigned lane_bytes = 0;
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       const int op = lane + 32 * k;
-      Job jb{nullptr, 0, 0, 0, 0, 1, 0u, 0};
+      Job jb{nullptr, 0, 0, 0, 0, 1, 0u, 0, false};
       if (op < Q) {
         const int slot = op;  // stage position op holds slot op (odd steps read opp(i) from it)
         const int cz = EVEN && !whole_row ? comp<L>(op, 2) : 0;
@@ -335,6 +365,7 @@ __global__ void __launch_bounds__(kTmaThreads, tma_min_blocks<L, K>())
         jb.es = sizeof(T);
         jb.dst = (unsigned)(((size_t)op * St::SEG + St::H - jb.hl) * sizeof(T));
         jb.kind = 1;
+        jb.gathered = by_rows && op < 4 * NG4;
       } else if (op < Q + St::NG) {
         if constexpr (NT == 1) {
           const int i = op - Q;
@@ -374,6 +405,23 @@ __global__ void __launch_bounds__(kTmaThreads, tma_min_blocks<L, K>())
       const int uy = jb.cy > 0 ? (y == 0 ? a.ny - 1 : y - 1) : (jb.cy < 0 ? (y == a.ny - 1 ? 0 : y + 1) : y);
       return jb.base + (size_t)(ux * plane + (long long)uy * a.nz) * jb.es;
     };
+    // The rows of lane k's four gathered slots for tile (x, y).
+    int gcx[4] = {0, 0, 0, 0}, gcy[4] = {0, 0, 0, 0};
+    if (lane < NG4) {
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        gcx[m] = comp<L>(4 * lane + m, 0);
+        gcy[m] = comp<L>(4 * lane + m, 1);
+      }
+    }
+    auto group_rows = [&](int x, int y, int (&r)[4]) {
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const int ux = gcx[m] > 0 ? (x == 0 ? a.nx - 1 : x - 1) : (gcx[m] < 0 ? (x == a.nx - 1 ? 0 : x + 1) : x);
+        const int uy = gcy[m] > 0 ? (y == 0 ? a.ny - 1 : y - 1) : (gcy[m] < 0 ? (y == a.ny - 1 ? 0 : y + 1) : y);
+        r[m] = (4 * lane + m) * a.nx * a.ny + ux * a.ny + uy;
+      }
+    };
     // With bulk_out the consumers leave a tile's results in its stage: each population and
     // tracer segment goes back to the row it came from (no halo then: odd steps read their own
     // row, even steps of one-tile rows the whole row), and the stage is refilled once the
@@ -391,10 +439,16 @@ __global__ void __launch_bounds__(kTmaThreads, tma_min_blocks<L, K>())
           if constexpr (NT == 1) tensor_store_2d(&maps.g, cell0, 0, st + St::off_trc);
         }
       } else {
+        if (by_rows && lane < NG4) {
+          int r[4];
+          group_rows(tws.x, tws.y, r);
+          tensor_scatter4(&maps.f, r[0], r[1], r[2], r[3],
+                          st + (size_t)4 * lane * St::SEG * sizeof(T));
+        }
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
           const Job& jb = jobs[k];
-          if (jb.kind == 1)
+          if (jb.kind == 1 && !jb.gathered)
             bulk_store(const_cast<unsigned char*>(job_row(jb, tws.x, tws.y)) +
                            (size_t)tws.zt * kTmaTile * jb.es,
                        st + jb.dst, (unsigned)(kTmaTile * jb.es));
@@ -426,10 +480,16 @@ __global__ void __launch_bounds__(kTmaThreads, tma_min_blocks<L, K>())
         tensor_copy_2d(st, &maps.f, cell0, 0, full + s);
         if constexpr (NT == 1) tensor_copy_2d(st + St::off_trc, &maps.g, cell0, 0, full + s);
       }
+      if (by_rows && lane < NG4) {
+        int r[4];
+        group_rows(x, y, r);
+        tensor_gather4(st + (size_t)4 * lane * St::SEG * sizeof(T), &maps.f, r[0], r[1], r[2],
+                       r[3], full + s);
+      }
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
         const Job& jb = jobs[k];
-        if (jb.kind == 1 && !by_map) {
+        if (jb.kind == 1 && !by_map && !jb.gathered) {
           copy_row_segment(st + jb.dst, job_row(jb, x, y), z0, jb.hl, jb.hr, a.nz, jb.es,
                            full + s);
         } else if (jb.kind == 2) {
