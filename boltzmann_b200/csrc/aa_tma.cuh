@@ -168,7 +168,10 @@ struct TmaStage {
   static constexpr int HG = EVEN && !WR ? 16 / (int)sizeof(Real) : 0;  // tracer halo
   static constexpr int SEG = kTmaTile + 2 * H;                   // populations per direction
   static constexpr int SEGG = kTmaTile + 2 * HG;
-  static constexpr size_t pop_bytes = (size_t)Q * SEG * sizeof(T);
+  // Even steps of one-tile rows move slots four rows at a time; the last group is padded with
+  // repeats of slot Q - 1 into rows Q .. QP - 1 of the stage.
+  static constexpr int QP = EVEN && WR ? 4 * ((Q + 3) / 4) : Q;
+  static constexpr size_t pop_bytes = (size_t)QP * SEG * sizeof(T);
   static constexpr size_t trc_bytes = (size_t)NG * SEGG * sizeof(Real);
   static constexpr size_t val_bytes = (size_t)kTmaTile * sizeof(Real);
   static constexpr size_t flag_bytes = kTmaTile;
@@ -225,6 +228,15 @@ struct StageSink {
         P::store_dev(p, val, weight<LL, Real>(i));
       else
         P::store(p, val, weight<LL, Real>(i));
+    }
+    if constexpr (EVEN && St::QP > LL::Q) {
+      // The padding rows of the last four-row group repeat slot Q - 1 (the store writes them
+      // to the same row again).
+      constexpr int i = LL::Q - 1;
+      const int pos = St::H + ((tid - comp<LL>(i, 2)) & (kTmaTile - 1));
+      const T w = base[i * St::SEG + pos];
+#pragma unroll
+      for (int r = LL::Q; r < St::QP; ++r) base[r * St::SEG + pos] = w;
     }
   }
   template <class TT, class TP, bool EVEN>
@@ -341,11 +353,11 @@ __global__ void __launch_bounds__(kTmaThreads, tma_min_blocks<L, K>())
       int kind;                   // 0 none, 1 row segment with halo, 2 own tile (no halo)
       bool gathered;              // moved by the four-row tensor copies instead (see below)
     };
-    // Even steps of one-tile rows: slots 0 .. 4 NG4 - 1 travel four rows at a time
+    // Even steps of one-tile rows: the population slots travel four rows at a time
     // (tile::gather4 / scatter4 over the population array seen as rows of 256 cells, row
-    // (slot, x, y)); lane k < NG4 moves slots 4k .. 4k + 3. The remaining slots keep their own
-    // copies.
-    constexpr int NG4 = EVEN && WR ? Q / 4 : 0;
+    // (slot, x, y)); lane k < NG4 moves slots 4k .. 4k + 3, the last group padded with repeats
+    // of slot Q - 1.
+    constexpr int NG4 = EVEN && WR ? St::QP / 4 : 0;
     const bool by_rows = NG4 > 0 && maps.use;
     Job jobs[2];
     unsigned lane_bytes = 0;
@@ -365,7 +377,7 @@ __global__ void __launch_bounds__(kTmaThreads, tma_min_blocks<L, K>())
         jb.es = sizeof(T);
         jb.dst = (unsigned)(((size_t)op * St::SEG + St::H - jb.hl) * sizeof(T));
         jb.kind = 1;
-        jb.gathered = by_rows && op < 4 * NG4;
+        jb.gathered = by_rows;
       } else if (op < Q + St::NG) {
         if constexpr (NT == 1) {
           const int i = op - Q;
@@ -394,8 +406,10 @@ __global__ void __launch_bounds__(kTmaThreads, tma_min_blocks<L, K>())
         jb.kind = 2;
       }
       jobs[k] = jb;
-      if (jb.kind != 0) lane_bytes += (unsigned)((kTmaTile + jb.hl + jb.hr) * jb.es);
+      if (jb.kind != 0 && !jb.gathered)
+        lane_bytes += (unsigned)((kTmaTile + jb.hl + jb.hr) * jb.es);
     }
+    if (by_rows && lane < NG4) lane_bytes += 4u * kTmaTile * (unsigned)sizeof(T);
     const unsigned expect = __reduce_add_sync(0xffffffffu, lane_bytes);
     const long long plane = (long long)a.ny * a.nz;
     // First byte of the row a job's segment of tile (x, y) comes from: the tile's own row, or
@@ -410,8 +424,9 @@ __global__ void __launch_bounds__(kTmaThreads, tma_min_blocks<L, K>())
     if (lane < NG4) {
 #pragma unroll
       for (int m = 0; m < 4; ++m) {
-        gcx[m] = comp<L>(4 * lane + m, 0);
-        gcy[m] = comp<L>(4 * lane + m, 1);
+        const int slot = 4 * lane + m < Q ? 4 * lane + m : Q - 1;
+        gcx[m] = comp<L>(slot, 0);
+        gcy[m] = comp<L>(slot, 1);
       }
     }
     auto group_rows = [&](int x, int y, int (&r)[4]) {
@@ -419,7 +434,8 @@ __global__ void __launch_bounds__(kTmaThreads, tma_min_blocks<L, K>())
       for (int m = 0; m < 4; ++m) {
         const int ux = gcx[m] > 0 ? (x == 0 ? a.nx - 1 : x - 1) : (gcx[m] < 0 ? (x == a.nx - 1 ? 0 : x + 1) : x);
         const int uy = gcy[m] > 0 ? (y == 0 ? a.ny - 1 : y - 1) : (gcy[m] < 0 ? (y == a.ny - 1 ? 0 : y + 1) : y);
-        r[m] = (4 * lane + m) * a.nx * a.ny + ux * a.ny + uy;
+        const int slot = 4 * lane + m < Q ? 4 * lane + m : Q - 1;
+        r[m] = slot * a.nx * a.ny + ux * a.ny + uy;
       }
     };
     // With bulk_out the consumers leave a tile's results in its stage: each population and
