@@ -56,6 +56,8 @@ StepArgs<Real> make_step_args(const lbm_sim& s, bool write_moments) {
     a.tr[t].g = static_cast<Real*>(s.tracers[t].g);
     a.tr[t].val = static_cast<Real*>(s.tracers[t].val);
     a.tr[t].omega = s.tracers[t].omega;
+    a.tr[t].omega_neg = s.tracers[t].omega_neg;
+    a.tr[t].trt = s.tracers[t].collision == 1;
   }
   a.write_moments = write_moments ? 1 : 0;
   a.path = s.kernel_path;

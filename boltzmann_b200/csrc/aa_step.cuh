@@ -39,7 +39,9 @@ template <class Real>
 struct TracerArgs {
   Real* g;    // [Qt][N]
   Real* val;  // [N]
-  Real omega;
+  Real omega;      // omega (BGK) or omega+ (TRT)
+  Real omega_neg;  // omega- (TRT)
+  int trt;
 };
 
 template <class Real>
@@ -349,7 +351,9 @@ __device__ __forceinline__ void moments_packed(float (&v)[L::Q], float& dr, floa
 }
 
 // Advection-diffusion update of one tracer cell in the fluid velocity u just computed
-// (src/lib.cl:102-189, 303-405), with its populations already loaded into g.
+// (src/lib.cl:102-189, 303-405), with its populations already loaded into g. TRT tracers take
+// the pair update of the fluid's TRT with their own rates, both 1 on fixed-value cells (the
+// D2Q5 / D3Q7 TRT kernels of python/boltzmann/kernel_gen.py:368-421).
 template <class TL, class TP, bool EVEN, class Real, class Sink = GlobalSink>
 __device__ __forceinline__ void tracer_update(const TracerArgs<Real>& tr, long long n,
                                               const CellPos& c, int flag, Real (&g)[TL::Q],
@@ -358,13 +362,16 @@ __device__ __forceinline__ void tracer_update(const TracerArgs<Real>& tr, long l
   Real rt = 0;
 #pragma unroll
   for (int i = 0; i < TL::Q; ++i) rt += g[i];
-  Real om = tr.omega;
+  Real om = tr.omega, om_n = tr.omega_neg;
   const bool tfixed = (flag & 8) != 0;  // FIXED_SCALAR_VALUE (src/lib.cl:156-161)
   if (tfixed) {
     om = 1;
+    om_n = 1;
     rt = tr.val[c.cell];
   }
-  if constexpr (sizeof(Real) == 4 && pack_collide<TL>())
+  if (tr.trt)
+    collide<TL, true, false>(g, rt, rt, u, uu, om, om_n);
+  else if constexpr (sizeof(Real) == 4 && pack_collide<TL>())
     collide_packed<TL, false, false>(g, rt, rt, u, uu, om, om);
   else
     collide<TL, false, false>(g, rt, rt, u, uu, om, om);

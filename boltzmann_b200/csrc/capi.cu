@@ -39,9 +39,11 @@ bool known_set(int d, int q) {
 // Sets that have a fluid update kernel (src/opencl.rs:123-129, plus D3Q27 TRT).
 bool fluid_kernel(int d, int q) { return (d == 2 && q == 9) || (d == 3 && q == 27); }
 
-// Sets that have a tracer update kernel: BGK D2Q5 / D3Q7 (src/opencl.rs:123-129).
+// Sets that have a tracer update kernel: D2Q5 / D3Q7 with BGK (src/opencl.rs:123-129) or TRT
+// (the kernels python/boltzmann/kernel_gen.py:250-462 generates, which the reference never
+// registers).
 bool tracer_kernel(int d, int q, int collision) {
-  return collision == LBM_BGK && ((d == 2 && q == 5) || (d == 3 && q == 7));
+  return (collision == LBM_BGK || collision == LBM_TRT) && ((d == 2 && q == 5) || (d == 3 && q == 7));
 }
 
 int activate(lbm_sim* s) {
@@ -216,7 +218,6 @@ int lbm_device_bytes(lbm_sim* sim, int64_t* out) {
 int lbm_add_tracer(lbm_sim* sim, int q, int collision, float omega_pos, float omega_neg,
                    int* out_index) {
   if (int rc = activate(sim)) return rc;
-  (void)omega_neg;
   if (!known_set(sim->dim, q))
     return fail(LBM_ERR_ARGUMENT,
                 "Unknown model: D" + std::to_string(sim->dim) + "Q" + std::to_string(q));
@@ -227,6 +228,7 @@ int lbm_add_tracer(lbm_sim* sim, int q, int collision, float omega_pos, float om
   t.q = q;
   t.collision = collision;
   t.omega = omega_pos;
+  t.omega_neg = omega_neg;
   const size_t rb = sim->real_bytes();
   LBM_CUDA(cudaMalloc(&t.g, (size_t)sim->n * q * rb));
   cudaError_t e = cudaMalloc(&t.val, (size_t)sim->n * rb);

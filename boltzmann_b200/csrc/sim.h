@@ -11,7 +11,8 @@ struct lbm_sim {
   struct Tracer {
     int q = 0;
     int collision = 0;
-    float omega = 0;
+    float omega = 0;      // omega (BGK) or omega+ (TRT)
+    float omega_neg = 0;  // omega- (TRT)
     void* g = nullptr;    // [q][N], float (double for F64 storage)
     void* val = nullptr;  // [N]
   };

@@ -87,7 +87,9 @@ LBM_API int lbm_device_bytes(lbm_sim* sim, int64_t* out);
 
 /* Adds an advection-diffusion tracer (g = 0, val = 0) and returns its index.
  * Replaces Scalar::new + Simulation::add_tracer (src/fields.rs:152-163,
- * src/simulation.rs:221-229). */
+ * src/simulation.rs:221-229). collision LBM_BGK (omega_pos) or LBM_TRT (omega_pos, omega_neg):
+ * the reference registers BGK tracer kernels only (src/opencl.rs:123-129); TRT follows the
+ * D2Q5 / D3Q7 kernels its generator writes (python/boltzmann/kernel_gen.py:250-462). */
 LBM_API int lbm_add_tracer(lbm_sim* sim, int q, int collision, float omega_pos, float omega_neg,
                    int* out_index);
 

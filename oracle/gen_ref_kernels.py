@@ -1,9 +1,9 @@
 """TEST INFRASTRUCTURE (the checker, never the product).
 
 Runs the reference's own sympy kernel generator (python/boltzmann/kernel_gen.py:250-462 of
-djbarker/boltzmann) to produce the D3Q27 TRT update kernel, which the reference can generate but
-never registers (src/opencl.rs:123-129). The output is written under oracle/_ref/gen/ and is
-never committed.
+djbarker/boltzmann) to produce the update kernels the reference can generate but never registers
+(src/opencl.rs:123-129): D3Q27 TRT for the fluid, D2Q5 and D3Q7 TRT for tracers. The output is
+written under oracle/_ref/gen/ and is never committed.
 
 kernel_gen imports boltzmann.core, which imports the compiled extension boltzmann.boltzmann
 (python/boltzmann/core.py:31). That extension cannot be built here (no Rust toolchain), so a
@@ -39,18 +39,23 @@ def generate(reference_root: Path, out_dir: Path) -> None:
     import boltzmann.kernel_gen as kg  # noqa: E402  (reference generator)
 
     out_dir.mkdir(parents=True, exist_ok=True)
-    src = kg.gen_kernel_AA_v1(kg.D3Q27, "fluid", "trt")
-    (out_dir / "update_d3q27_trt.cl").write_text(src + "\n")
+    for model, kind, name in ((kg.D3Q27, "fluid", "update_d3q27_trt"),
+                              (kg.D2Q5, "scalar", "update_d2q5_trt"),
+                              (kg.D3Q7, "scalar", "update_d3q7_trt")):
+        (out_dir / f"{name}.cl").write_text(kg.gen_kernel_AA_v1(model, kind, "trt") + "\n")
 
-    # Self-check of the generator: its D2Q9 TRT must equal lib.cl's update_d2q9_trt up to
-    # whitespace (the reference's own kernel was produced this way).
-    gen_d2q9 = kg.gen_kernel_AA_v1(kg.D2Q9, "fluid", "trt")
+    # Self-checks of the generator against the kernels lib.cl registers (the reference's own
+    # kernels were produced this way): each generated kernel must equal, up to whitespace, the
+    # text of lib.cl from that kernel's first line on.
     lib = (reference_root / "src" / "lib.cl").read_text()
-    start = lib.index("kernel void update_d2q9_trt")
-    in_lib = lib[start:]
     squash = lambda s: re.sub(r"\s+", "", s)  # noqa: E731
-    if squash(gen_d2q9) != squash(in_lib):
-        raise SystemExit("kernel_gen D2Q9 TRT differs from lib.cl update_d2q9_trt")
+    for model, kind, omega, name in ((kg.D2Q9, "fluid", "trt", "update_d2q9_trt"),
+                                     (kg.D2Q5, "scalar", "bgk", "update_d2q5_bgk"),
+                                     (kg.D3Q7, "scalar", "bgk", "update_d3q7_bgk")):
+        gen = kg.gen_kernel_AA_v1(model, kind, omega)
+        in_lib = lib[lib.index("kernel void " + name):]
+        if not squash(in_lib).startswith(squash(gen)):
+            raise SystemExit(f"kernel_gen output differs from lib.cl {name}")
 
 
 if __name__ == "__main__":

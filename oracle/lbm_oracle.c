@@ -6,7 +6,7 @@
  * A table-driven C restatement of the reference's hot path (djbarker/boltzmann):
  *   - equilibrium initialisation, src/velocities.rs:43-52 (FP32, same operation order);
  *   - the AA-pattern fused stream+collide kernels of src/lib.cl (D2Q9/D3Q27 BGK, D2Q9 TRT,
- *     D2Q5/D3Q7 advection-diffusion) and the D3Q27 TRT kernel its generator
+ *     D2Q5/D3Q7 advection-diffusion) and the D3Q27 TRT and D2Q5/D3Q7 TRT kernels its generator
  *     python/boltzmann/kernel_gen.py:250-462 writes, as one generic routine over a velocity set;
  *   - the constant and Boussinesq acceleration passes, src/lib.cl:14-44 and 60-92;
  *   - the host step loop, src/simulation.rs:278-446.

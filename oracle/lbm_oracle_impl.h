@@ -127,12 +127,15 @@ static void FN(fluid_cell)(const FN(fluid_t) * a, long x, long y, long z, int ev
 
 typedef struct {
   FN(grid_t) g;
-  REAL om;
+  int trt;
+  REAL om, om_neg; /* omega (BGK) or omega+, omega- (TRT) */
   REAL *f, *val;
   const REAL* vel; /* the fluid velocity written this step */
 } FN(tracer_t);
 
-/* One tracer cell: src/lib.cl:102-189 (D2Q5), 303-405 (D3Q7). */
+/* One tracer cell: src/lib.cl:102-189 (D2Q5 BGK), 303-405 (D3Q7 BGK); TRT as the reference's
+ * generator writes it for a scalar (python/boltzmann/kernel_gen.py:368-421: the fixed-value
+ * override sets both rates to 1, then the pair update of the fluid's TRT). */
 static void FN(tracer_cell)(const FN(tracer_t) * a, long x, long y, long z, int even) {
   const FN(grid_t)* g = &a->g;
   const int q = g->lat.q, d = g->dim;
@@ -148,16 +151,31 @@ static void FN(tracer_cell)(const FN(tracer_t) * a, long x, long y, long z, int 
   REAL r = 0, v[3] = {0, 0, 0};
   for (int i = 0; i < q; ++i) r += fl[i];
   for (int k = 0; k < d; ++k) v[k] = a->vel[cell * d + k];
-  REAL om = a->om;
+  REAL om = a->om, om_n = a->om_neg;
   if (fixed) { /* src/lib.cl:156-161 */
     om = 1;
+    om_n = 1;
     r = a->val[cell];
   }
   REAL vv = 0;
   for (int k = 0; k < d; ++k) vv += v[k] * v[k];
   const double rd = r, vvd = vv, vd[3] = {v[0], v[1], v[2]};
-  for (int i = 0; i < q; ++i)
-    fl[i] = (REAL)((double)fl[i] + (double)om * (FN(feq)(g, i, rd, vd, vvd) - (double)fl[i]));
+  if (!a->trt) {
+    for (int i = 0; i < q; ++i)
+      fl[i] = (REAL)((double)fl[i] + (double)om * (FN(feq)(g, i, rd, vd, vvd) - (double)fl[i]));
+  } else {
+    for (int i = 0; i < q; ++i) {
+      const int j = g->lat.opp[i];
+      if (j < i) continue;
+      const double fe_i = FN(feq)(g, i, rd, vd, vvd), fe_j = FN(feq)(g, j, rd, vd, vvd);
+      const double sym = (double)(REAL)(fl[i] + fl[j]) * 0.5;
+      const double asym = (double)(REAL)(fl[i] - fl[j]) * 0.5;
+      const double fpos = (double)om * ((fe_i + fe_j) * 0.5 - sym);
+      const double fneg = (double)om_n * ((fe_i - fe_j) * 0.5 - asym);
+      fl[i] = (REAL)((double)fl[i] + (fpos + fneg));
+      if (j != i) fl[j] = (REAL)((double)fl[j] + (fpos - fneg));
+    }
+  }
 
   FN(aa_store)(g, a->f, cell, even, fl, at);
   a->val[cell] = r; /* src/lib.cl:188 */
@@ -181,8 +199,9 @@ int FN(lbm_oracle_iterate)(int dim, const int64_t* counts, const int32_t* flags,
                            REAL* acc, int use_acc, const REAL* gravity, int ncouplings,
                            const int32_t* c_tracer, const REAL* c_alpha, const REAL* c_c0,
                            const REAL* c_g, int ntracers, const int32_t* t_q,
-                           const int32_t* t_collision, const REAL* t_om, REAL* const* t_g,
-                           REAL* const* t_C, int64_t iters, int nthreads) {
+                           const int32_t* t_collision, const REAL* t_om,
+                           const REAL* t_om_neg, REAL* const* t_g, REAL* const* t_C,
+                           int64_t iters, int nthreads) {
   if (iters % 2 != 0) { /* src/simulation.rs:279-281 */
     g_err = "iters must be even";
     return 1;
@@ -210,13 +229,16 @@ int FN(lbm_oracle_iterate)(int dim, const int64_t* counts, const int32_t* flags,
     return 1;
   }
   for (int t = 0; t < ntracers; ++t) {
-    const int ok = t_collision[t] == 0 && ((dim == 2 && t_q[t] == 5) || (dim == 3 && t_q[t] == 7));
+    const int ok = (t_collision[t] == 0 || t_collision[t] == 1) &&
+                   ((dim == 2 && t_q[t] == 5) || (dim == 3 && t_q[t] == 7));
     if (!ok) {
       g_err = "Kernel not found (tracer)";
       return 1;
     }
     FN(make_grid)(&ta[t].g, dim, counts, flags, t_q[t]);
+    ta[t].trt = t_collision[t] == 1;
     ta[t].om = t_om[t];
+    ta[t].om_neg = t_om_neg[t];
     ta[t].f = t_g[t];
     ta[t].val = t_C[t];
     ta[t].vel = vel;

@@ -193,6 +193,7 @@ class OracleSimulation:
         t_q = arr_i([t.q for t in tr] or [0])
         t_col = arr_i([t.omega.kind for t in tr] or [0])
         t_om = arr_r([t.omega.pos for t in tr] or [0])
+        t_om_neg = arr_r([t.omega.neg for t in tr] or [0])
         t_g = (C.c_void_p * max(ntr, 1))(*[t.g.ctypes.data for t in tr])
         t_C = (C.c_void_p * max(ntr, 1))(*[t.val.ctypes.data for t in tr])
         counts = np.asarray(self.counts, np.int64)
@@ -230,6 +231,7 @@ class OracleSimulation:
             _ptr(t_q),
             _ptr(t_col),
             _ptr(t_om),
+            _ptr(t_om_neg),
             t_g,
             t_C,
             C.c_int64(iters),

@@ -3,9 +3,10 @@
  *
  * Host loop around the reference's own OpenCL kernels, compiled as C++:
  *   - src/lib.cl (djbarker/boltzmann), included unmodified from the reference tree;
- *   - update_d3q27_trt, which the reference never registers (src/opencl.rs:123-129) but whose
- *     source its generator python/boltzmann/kernel_gen.py:250-462 produces; oracle/build.py
- *     writes it to oracle/_ref/gen/ at build time.
+ *   - update_d3q27_trt, update_d2q5_trt and update_d3q7_trt, which the reference never
+ *     registers (src/opencl.rs:123-129) but whose source its generator
+ *     python/boltzmann/kernel_gen.py:250-462 produces; oracle/build.py writes them to
+ *     oracle/_ref/gen/ at build time.
  *
  * The loop restates Simulation::iterate (src/simulation.rs:278-446): the constant-acceleration
  * pass once per call, then per step every Boussinesq pass (last one wins), the fluid kernel,
@@ -26,6 +27,8 @@
 
 #include "lib.cl"
 #include "update_d3q27_trt.cl"
+#include "update_d2q5_trt.cl"
+#include "update_d3q7_trt.cl"
 
 namespace {
 
@@ -64,13 +67,15 @@ const char* lbm_ref_last_error(void) { return g_err.c_str(); }
 /* One call == Simulation::iterate(iters) after the upload (src/simulation.rs:278-446).
  * Arrays are the reference's host layouts: f [N, q], rho [N], vel [N, dim], acc [N, dim],
  * tracer g [N, q_t], C [N]; N = prod(counts) in row-major order (x slowest).
- * collision: 0 = BGK, 1 = TRT. */
+ * collision (fluid and each tracer): 0 = BGK, 1 = TRT; a tracer's rates are t_om (omega or
+ * omega+) and t_om_neg. */
 int lbm_ref_iterate(int dim, const int64_t* counts, int32_t* flags, int q, int collision,
                     float om_pos, float om_neg, float* f, float* rho, float* vel, float* acc,
                     int use_acc, const float* gravity, int ncouplings, const int32_t* c_tracer,
                     const float* c_alpha, const float* c_c0, const float* c_g, int ntracers,
                     const int32_t* t_q, const int32_t* t_collision, const float* t_om,
-                    float* const* t_g, float* const* t_C, int64_t iters, int nthreads) {
+                    const float* t_om_neg, float* const* t_g, float* const* t_C, int64_t iters,
+                    int nthreads) {
   if (iters % 2 != 0) return fail("iters must be even");
   if (dim < 2 || dim > 3) return fail("no update kernel for this dimension");
   if (nthreads <= 0) nthreads = omp_get_max_threads();
@@ -83,7 +88,8 @@ int lbm_ref_iterate(int dim, const int64_t* counts, int32_t* flags, int q, int c
   const bool fluid_ok = (dim == 2 && q == 9) || (dim == 3 && q == 27);
   if (!fluid_ok) return fail("Kernel not found (fluid)");
   for (int t = 0; t < ntracers; ++t) {
-    const bool ok = t_collision[t] == 0 && ((dim == 2 && t_q[t] == 5) || (dim == 3 && t_q[t] == 7));
+    const bool ok = (t_collision[t] == 0 || t_collision[t] == 1) &&
+                    ((dim == 2 && t_q[t] == 5) || (dim == 3 && t_q[t] == 7));
     if (!ok) return fail("Kernel not found (tracer)");
   }
 
@@ -134,13 +140,19 @@ int lbm_ref_iterate(int dim, const int64_t* counts, int32_t* flags, int q, int c
     for (int t = 0; t < ntracers; ++t) {
       float* g = t_g[t];
       float* C = t_C[t];
-      float om = t_om[t];
-      if (dim == 2)
+      float om = t_om[t], om_n = t_om_neg[t];
+      if (t_collision[t] == 0 && dim == 2)
         for_each_work_item(dim, s, nthreads,
                            [&] { update_d2q5_bgk(s, even, om, g, C, vel, flags); });
-      else
+      else if (t_collision[t] == 0)
         for_each_work_item(dim, s, nthreads,
                            [&] { update_d3q7_bgk(s, even, om, g, C, vel, flags); });
+      else if (dim == 2)
+        for_each_work_item(dim, s, nthreads,
+                           [&] { update_d2q5_trt(s, even, om, om_n, g, C, vel, flags); });
+      else
+        for_each_work_item(dim, s, nthreads,
+                           [&] { update_d3q7_trt(s, even, om, om_n, g, C, vel, flags); });
     }
   }
   return 0;

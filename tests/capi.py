@@ -54,10 +54,12 @@ class CApiSim:
             _lib.lbm_destroy(self.h)
             self.h = None
 
-    def add_tracer(self, om: float, q=None) -> int:
+    def add_tracer(self, om: float, q=None, kind: int = 0, om_neg: float = 0.0) -> int:
+        """kind 0: BGK with om; 1: TRT with (om, om_neg)."""
         idx = C.c_int()
         tq = q or {2: 5, 3: 7}[self.d]
-        check(_lib.lbm_add_tracer(self.h, tq, 0, C.c_float(om), C.c_float(0), C.byref(idx)))
+        check(_lib.lbm_add_tracer(self.h, tq, kind, C.c_float(om), C.c_float(om_neg),
+                                  C.byref(idx)))
         self.vals.append(np.zeros(self.counts, np.float32))
         self.tq.append(tq)
         return idx.value

@@ -7,7 +7,8 @@ case spec, the seeded inputs and the outputs after every ``iterate`` call, so la
 neither the reference tree nor the RNG.
 
 Run from the repository root where the reference tree exists:
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]
+Cases take their seeds from their position in CASES, so new cases go at the end.
 """
 
 from __future__ import annotations
@@ -60,6 +61,23 @@ CASES: dict[str, dict] = {
         walls=True,
         tracers=[["t0", ["bgk", 0.65]]],
         couplings=[["t0", 0.1, 0.5, [0.0, 0.0, -0.01]]],
+        calls=[4],
+    ),
+    # TRT tracers: the D2Q5 / D3Q7 TRT kernels the reference's generator writes
+    # (python/boltzmann/kernel_gen.py:250-462) but src/opencl.rs never registers.
+    "d2q9_trt_trt_tracer": dict(
+        counts=[16, 12],
+        omega=["trt", 0.57],
+        walls=True,
+        tracers=[["t0", ["trt", 0.62]]],
+        couplings=[["t0", 0.1, 0.5, [0.0, -0.01]]],
+        calls=[4, 6],
+    ),
+    "d3q27_bgk_trt_tracer": dict(
+        counts=[6, 5, 7],
+        omega=["bgk", 0.6],
+        walls=True,
+        tracers=[["t0", ["trt", 0.66]]],
         calls=[4],
     ),
 }
@@ -118,11 +136,13 @@ def run_oracle(spec: dict, inputs: dict, backend: str) -> list[dict[str, np.ndar
     return outs
 
 
-def main() -> None:
+def main(only: list[str]) -> None:
     if oracle_build.build_ref() is None:
         raise SystemExit("the reference tree is needed to generate golden fixtures")
     oracle_build.build_oracle()
     for k, (name, spec) in enumerate(CASES.items()):
+        if only and name not in only:
+            continue
         inputs = seeded_inputs(spec, seed=k)
         outs = run_oracle(spec, inputs, backend="reference")
         arrays = {f"in_{key}": v for key, v in inputs.items()}
@@ -133,4 +153,4 @@ def main() -> None:
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])  # case names; none: every case

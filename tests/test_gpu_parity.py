@@ -44,7 +44,8 @@ def _capi_from_spec(spec, inputs, storage="f32", path="auto"):
     sim.vel[...] = inputs["vel"]
     index = {}
     for name, om in spec.get("tracers", []):
-        t = sim.add_tracer(_omega_args(om)[1])
+        tk, tpos, tneg = _omega_args(om)
+        t = sim.add_tracer(tpos, kind=tk, om_neg=tneg)
         sim.vals[t][...] = inputs[f"val_{name}"]
         index[name] = t
     if spec.get("gravity") is not None:
@@ -336,6 +337,10 @@ TMA_CASES = {
                                       tracers=[["t0", ["bgk", 0.65]]],
                                       couplings=[["t0", 0.1, 0.5, [0.0, 0.0, -0.01]]], calls=[4]),
     "d3q27_single_row": dict(counts=[1, 1, 512], omega=["bgk", 0.6], calls=[2]),
+    "d3q27_bgk_trt_tracer_coupling": dict(counts=[3, 4, 256], omega=["bgk", 0.6], walls=True,
+                                          tracers=[["t0", ["trt", 0.64]]],
+                                          couplings=[["t0", 0.1, 0.5, [0.0, 0.0, -0.01]]],
+                                          calls=[2, 4]),
 }
 
 
