@@ -277,7 +277,6 @@ __global__ void __launch_bounds__(kTmaThreads, tma_min_blocks<L, K>())
   using TL = typename TracerLattice<L::D>::type;
   using St = TmaStage<L, K, NT, EVEN, WR>;
   constexpr int Q = L::Q;
-  constexpr int NOPS = Q + St::NG + 2;  // copy jobs per tile: populations, tracer, value, flags
 
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)S * St::bytes);
@@ -324,8 +323,8 @@ __global__ void __launch_bounds__(kTmaThreads, tma_min_blocks<L, K>())
   // segments before refilling it (bulk stores). Other even steps store from registers (their
   // results' segments are shifted by c_iz, so not 16-byte aligned) and release the stage warp by
   // warp as soon as the operands are read. (Bulk stores of the aligned part with plain stores
-  // of the two partial chunks per slot were correct there but made the producer the limit:
-  // -8% with FP32, -17% with FP16 populations on the 4096x2048 channel.)
+  // of the two partial chunks per slot were correct there but made the producer the limit on
+  // the 4096x2048 channel: no gain with FP32 populations, 8-17% slower with FP16.)
   constexpr bool whole_row = WR;
   constexpr bool bulk_out = !EVEN || WR;
   if (tid == 0) {
