@@ -985,6 +985,20 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   const uint32_t idesc = umma_idesc_bf16(128, 32);
   const unsigned a1c_addr = smem_addr(a1c), w2c_addr = smem_addr(w2c);
   bool healthy = true;
+  // Layer-1 A fragments: element e of k-step kk holds input k = 16 kk + 2 tq + 8 (e >> 1), that
+  // is tap k / 4 and the channel pair (k & 3) / 2 of the feature cell shifted by the tap. The
+  // offset of that word from the cell's own (in 32-bit words of the feature region) depends on
+  // the lane only; taps past 8 are the K padding (zero).
+  int l1off[3][2];
+  unsigned l1valid = 0;
+#pragma unroll
+  for (int kk = 0; kk < 3; ++kk)
+#pragma unroll
+    for (int hi = 0; hi < 2; ++hi) {
+      const int k = kk * 16 + 2 * tq + 8 * hi, tap = k >> 2;
+      l1off[kk][hi] = 2 * ((tap / 3 - 1) * kXC + tap % 3 - 1) + ((k & 3) >> 1);
+      if (tap < 9) l1valid |= 1u << (2 * kk + hi);
+    }
   unsigned phase = 0;
 
   const int ntiles = f.tiles_x * f.tiles_y;
@@ -1047,12 +1061,13 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     // Layer 1 on [x0 - 2, ..) x [y0 - 2, ..): A fragments gathered from the features by tap.
     constexpr int n1 = kA1R * kA1C;
     for (int mt = warp; mt * 16 < n1; mt += kWarps) {
-      int rq[2], cq[2];
+      int rq[2], cq[2], xw[2];  // xw: word index of the cell in the feature region
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int q = min(mt * 16 + gq + 8 * h, n1 - 1);
         rq[h] = q / kA1C;
         cq[h] = q - rq[h] * kA1C;
+        xw[h] = 2 * ((rq[h] + 1) * kXC + cq[h] + 1);
       }
       float acc[4][4];
 #pragma unroll
@@ -1064,12 +1079,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         uint32_t a[4];
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
-          const int h = e & 1, k = kk * 16 + 2 * tq + (e >> 1) * 8, tap = k >> 2;
-          a[e] = 0u;
-          if (tap < 9) {
-            const int xi = (rq[h] + 1 + tap / 3 - 1) * kXC + cq[h] + 1 + tap % 3 - 1;
-            a[e] = xs[2 * xi + ((k & 3) >> 1)];
-          }
+          const int h = e & 1, hi = e >> 1;
+          a[e] = (l1valid >> (2 * kk + hi)) & 1u ? xs[xw[h] + l1off[kk][hi]] : 0u;
         }
         uint32_t bfr[4][2];
 #pragma unroll
