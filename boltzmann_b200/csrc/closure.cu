@@ -1002,18 +1002,20 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   unsigned phase = 0;
 
   const int ntiles = f.tiles_x * f.tiles_y;
-  for (int t = blockIdx.x; t < ntiles && healthy; t += gridDim.x) {
+  // Raw fields and features of tile t (the raw fields pass through the layer-2 area, which is
+  // free from a tile's layer 3 until the next tile's epilogue), by warps 1 .. 15: warp 0 issues
+  // the layer-2 MMAs meanwhile. Named barrier 1 orders the staging before the features.
+  constexpr int kStageThreads = kFusedThreads - 32;
+  auto stage_features = [&](int t) {
+    if (warp == 0) return;
+    const int st = threadIdx.x - 32;
     const int64_t x0 = (int64_t)(t / f.tiles_y) * kFR, y0 = (int64_t)(t % f.tiles_y) * kFC;
-    tc_fence_before();
-    __syncthreads();  // the previous tile is done with every region and every TMEM column
-    tc_fence_after();
-
     // Raw fields on [x0 - 4, x0 + kFR + 4) x [y0 - 4, y0 + kFC + 4), staged with coalesced loads
-    // into the layer-2 area (free until layer 2 runs); velocities on walls read as 0.
+    // into the layer-2 area; velocities on walls read as 0.
     float* raw_rho = reinterpret_cast<float*>(a2s);
     float2* raw_vel = reinterpret_cast<float2*>(raw_rho + kRawR * kRawC);
     int* raw_flag = reinterpret_cast<int*>(raw_vel + kRawR * kRawC);
-    for (int i = threadIdx.x; i < kRawR * kRawC; i += blockDim.x) {
+    for (int i = st; i < kRawR * kRawC; i += kStageThreads) {
       const int r = i / kRawC, c = i - r * kRawC;
       const int64_t x = x0 - 4 + r, y = y0 - 4 + c;
       float rv = 0.0f;
@@ -1029,10 +1031,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       raw_vel[i] = vv;
       raw_flag[i] = fl;
     }
-    __syncthreads();
+    asm volatile("bar.sync 1, %0;" ::"r"(kStageThreads) : "memory");
     // Features on [x0 - 3, x0 + kFR + 3) x [y0 - 3, y0 + kFC + 3), the arithmetic of
     // cell_features (np.gradient edges, walls at rest, normalise, BF16) on the staged fields.
-    for (int i = threadIdx.x; i < kXR * kXC; i += blockDim.x) {
+    for (int i = st; i < kXR * kXC; i += kStageThreads) {
       const int r = i / kXC, c = i - r * kXC;
       const int64_t x = x0 - 3 + r, y = y0 - 3 + c;
       uint2 packed = make_uint2(0, 0);
@@ -1056,7 +1058,15 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       xs[2 * i] = packed.x;
       xs[2 * i + 1] = packed.y;
     }
-    __syncthreads();
+  };
+  // Tile t's layer-2 MMAs run while the CTA stages and featurises its next tile.
+  if ((int)blockIdx.x < ntiles) stage_features(blockIdx.x);
+  for (int t = blockIdx.x; t < ntiles && healthy; t += gridDim.x) {
+    const int64_t x0 = (int64_t)(t / f.tiles_y) * kFR, y0 = (int64_t)(t % f.tiles_y) * kFC;
+    tc_fence_before();
+    __syncthreads();  // tile t's features are in place; the previous tile is done with a1c, a2s
+                      // and every TMEM column
+    tc_fence_after();
 
     // Layer 1 on [x0 - 2, ..) x [y0 - 2, ..): A fragments gathered from the features by tap.
     constexpr int n1 = kA1R * kA1C;
@@ -1140,6 +1150,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       }
       umma_commit(mma_done);
     }
+    if (t + (int)gridDim.x < ntiles) stage_features(t + gridDim.x);
     const bool got = cl_mbar_wait(mma_done, phase);
     phase ^= 1u;
     if (!__syncthreads_and(got)) {
