@@ -37,7 +37,8 @@ NVCC_FLAGS = [
 ]
 
 CUDA_SOURCES = ["aa_d2q9.cu", "aa_d3q27.cu", "fields.cu", "capi.cu", "noalloc.cu", "ensemble.cu", "closure.cu"]
-HEADERS = ["aa_step.cuh", "aa_tma.cuh", "aa_launch.cuh", "lattice.cuh", "storage.cuh", "sim.h"]
+HEADERS = ["aa_step.cuh", "aa_tma.cuh", "aa_pair.cuh", "aa_launch.cuh", "lattice.cuh",
+           "storage.cuh", "sim.h"]
 
 
 def _run(cmd: list[str]) -> None:

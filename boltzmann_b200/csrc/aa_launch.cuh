@@ -144,14 +144,19 @@ template <class L, bool TRT, int K, bool EVEN, int NT, bool WR>
 cudaError_t launch_tma(const StepArgs<typename Pop<K>::real>& a, cudaStream_t stream) {
   constexpr int S = tma_stages<L, K, NT, EVEN, WR>();
   constexpr size_t smem = tma_smem_bytes<L, K, NT, EVEN, S, WR>();
-  auto kern = aa_tma_kernel<L, TRT, K, EVEN, NT, S, WR>;
+  // Two cells a consumer thread: D3Q27 BGK with 16-bit populations and no tracer, on the steps
+  // whose results go back through the stage. (TRT needs more than the 128 registers three CTAs
+  // a SM leave a thread, and spills.)
+  constexpr bool PAIR = L::Q >= 27 && !TRT && dev_in<K>() && NT == 0 && (!EVEN || WR);
+  constexpr int threads = tma_threads<PAIR>();
+  auto kern = aa_tma_kernel<L, TRT, K, EVEN, NT, S, WR, PAIR>;
   static std::once_flag once;
   static cudaError_t setup_err = cudaSuccess;
   static int per_sm = 1;
   std::call_once(once, [&] {
     setup_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (setup_err == cudaSuccess)
-      setup_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTmaThreads, smem);
+      setup_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
     if (per_sm < 1) per_sm = 1;
   });
   if (setup_err != cudaSuccess) return setup_err;
@@ -173,7 +178,7 @@ cudaError_t launch_tma(const StepArgs<typename Pop<K>::real>& a, cudaStream_t st
       ok = ok && encode_slot_map<Real>(&maps.g, a.tr[0].g, a.n, TracerLattice<L::D>::type::Q);
     maps.use = ok ? 1 : 0;
   }
-  kern<<<(unsigned)grid, kTmaThreads, smem, stream>>>(a, maps);
+  kern<<<(unsigned)grid, threads, smem, stream>>>(a, maps);
   return cudaGetLastError();
 }
 

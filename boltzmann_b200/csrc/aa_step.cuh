@@ -202,6 +202,12 @@ __device__ __forceinline__ void collide(Real (&v)[L::Q], Real r, Real dr, const 
   }
 }
 
+// Fused multiply-add in the compute precision, written out so that the operation sequence of the
+// FP32 cell update is fixed in the source (the two-cells-a-thread path repeats it lane for lane
+// on packed instructions and must round identically).
+__device__ __forceinline__ float fma_r(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_r(double a, double b, double c) { return fma(a, b, c); }
+
 // ---- Packed FP32 (Blackwell FADD2 / FMUL2 / FFMA2): two independent FP32 operations per
 // instruction, each lane rounded exactly as the scalar operation (round to nearest even).
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
@@ -235,20 +241,21 @@ __device__ __forceinline__ void collide_packed(float (&v)[L::Q], float r, float 
   constexpr int P = (L::Q - 1) / 2;
   const float ru = over_den<L>(r);
   const float unit = DEV ? over_den<L>(dr) : ru;
-  const float quad = -1.5f * uu;
+  const float quad = __fmul_rn(-1.5f, uu);
   {
     const float k0 = float(L::wk(0));
-    const float e0 = k0 * ru * quad + (k0 * unit + (DEV ? weight_gap<L, float>(0) : 0.0f));
-    v[0] += om_pos * (e0 - v[0]);
+    const float e0 = __fmaf_rn(__fmul_rn(k0, ru), quad,
+                               __fmaf_rn(k0, unit, DEV ? weight_gap<L, float>(0) : 0.0f));
+    v[0] = __fmaf_rn(om_pos, __fsub_rn(e0, v[0]), v[0]);
   }
 #pragma unroll
   for (int p = 0; p + 1 < P; p += 2) {
     const int i = 2 * p + 1, j = 2 * p + 3;
     const float ki = float(L::wk(i)), kj = float(L::wk(j));
     const float2 cu = make_float2(c_dot<L>(i, u), c_dot<L>(j, u));
-    const float2 kru = make_float2(ki * ru, kj * ru);
-    const float2 ku = make_float2(ki * unit + (DEV ? weight_gap<L, float>(i) : 0.0f),
-                                  kj * unit + (DEV ? weight_gap<L, float>(j) : 0.0f));
+    const float2 kru = make_float2(__fmul_rn(ki, ru), __fmul_rn(kj, ru));
+    const float2 ku = make_float2(__fmaf_rn(ki, unit, DEV ? weight_gap<L, float>(i) : 0.0f),
+                                  __fmaf_rn(kj, unit, DEV ? weight_gap<L, float>(j) : 0.0f));
     const float2 X = fma2(mul2(splat(4.5f), cu), cu, splat(quad));
     const float2 A = fma2(kru, X, ku);
     const float2 B = mul2(mul2(kru, splat(3.0f)), cu);
@@ -273,19 +280,20 @@ __device__ __forceinline__ void collide_packed(float (&v)[L::Q], float r, float 
     constexpr int i = 2 * (P - 1) + 1;
     const float cu = c_dot<L>(i, u);
     const float k = float(L::wk(i));
-    const float A =
-        k * ru * (quad + 4.5f * cu * cu) + (k * unit + (DEV ? weight_gap<L, float>(i) : 0.0f));
-    const float B = k * ru * 3.0f * cu;
+    const float kr = __fmul_rn(k, ru);
+    const float X = __fmaf_rn(__fmul_rn(4.5f, cu), cu, quad);
+    const float A = __fmaf_rn(kr, X, __fmaf_rn(k, unit, DEV ? weight_gap<L, float>(i) : 0.0f));
+    const float B = __fmul_rn(__fmul_rn(kr, 3.0f), cu);
     if constexpr (TRT) {
-      const float sp = 0.5f * (v[i] + v[i + 1]);
-      const float dp = 0.5f * (v[i] - v[i + 1]);
-      const float fp = om_pos * (A - sp);
-      const float fn = om_neg * (B - dp);
-      v[i] += fp + fn;
-      v[i + 1] += fp - fn;
+      const float sp = __fmul_rn(0.5f, __fadd_rn(v[i], v[i + 1]));
+      const float dp = __fmul_rn(0.5f, __fsub_rn(v[i], v[i + 1]));
+      const float fp = __fmul_rn(om_pos, __fsub_rn(A, sp));
+      const float fn = __fmul_rn(om_neg, __fsub_rn(B, dp));
+      v[i] = __fadd_rn(v[i], __fadd_rn(fp, fn));
+      v[i + 1] = __fadd_rn(v[i + 1], __fsub_rn(fp, fn));
     } else {
-      v[i] += om_pos * (A + B - v[i]);
-      v[i + 1] += om_pos * (A - B - v[i + 1]);
+      v[i] = __fmaf_rn(om_pos, __fsub_rn(__fadd_rn(A, B), v[i]), v[i]);
+      v[i + 1] = __fmaf_rn(om_pos, __fsub_rn(__fsub_rn(A, B), v[i + 1]), v[i + 1]);
     }
   }
 }
@@ -470,7 +478,7 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
   } else if (a.acc_mode == kAccBoussinesq) {
     const Real b = a.alpha * (cval - a.c0);  // src/lib.cl:71
 #pragma unroll
-    for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] += b * a.force[ax];
+    for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] = fma_r(b, a.force[ax], u[ax]);
   }
   const bool fixed = (flag & 6) != 0;  // FIXED_FLUID_VELOCITY | FIXED_FLUID_DENSITY
   if (fixed) {                         // src/lib.cl:257-262
@@ -481,9 +489,9 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
 #pragma unroll
     for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] = a.vel[(size_t)c.cell * L::D + ax - (3 - L::D)];
   }
-  Real uu = 0;
+  Real uu = u[3 - L::D] * u[3 - L::D];
 #pragma unroll
-  for (int ax = 3 - L::D; ax < 3; ++ax) uu += u[ax] * u[ax];
+  for (int ax = 4 - L::D; ax < 3; ++ax) uu = fma_r(u[ax], u[ax], uu);
 
   if constexpr (sizeof(Real) == 4 && pack_collide<L>())
     collide_packed<L, TRT, true>(f, r, dr, u, uu, om_pos, om_neg);

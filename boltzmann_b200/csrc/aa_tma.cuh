@@ -35,6 +35,7 @@
 
 #include <cstdint>
 
+#include "aa_pair.cuh"
 #include "aa_step.cuh"
 
 namespace lbm {
@@ -255,20 +256,30 @@ struct StageSink {
 
 constexpr int kConsumerWarps = kTmaTile / 32;
 constexpr int kTmaThreads = kTmaTile + 32;  // + one producer warp
+// PAIR: each consumer thread updates two cells of the tile (tid and tid + 128), with half the
+// consumer warps.
+template <bool PAIR>
+__host__ __device__ constexpr int tma_consumer_warps() {
+  return PAIR ? kConsumerWarps / 2 : kConsumerWarps;
+}
+template <bool PAIR>
+__host__ __device__ constexpr int tma_threads() {
+  return 32 * tma_consumer_warps<PAIR>() + 32;
+}
 
 // CTAs per SM the register allocation is asked to allow. 32- and 64-bit populations: one, so
 // the compiler keeps more of each cell in registers (~90 for FP32 D3Q27, ~80 for the fused
 // D2Q9 + tracer even step) and two CTAs share an SM; measured 3-5% faster than three leaner CTAs.
 // 16-bit populations move half the bytes and need the occupancy instead: three CTAs for D3Q27,
 // four for D2Q9 (one CTA a SM cost them 15%).
-template <class L, int K>
+template <class L, int K, bool PAIR = false>
 constexpr int tma_min_blocks() {
-  return (K == kF16 || K == kBF16) ? (L::Q >= 27 ? 3 : 4) : 1;
+  return PAIR ? 3 : ((K == kF16 || K == kBF16) ? (L::Q >= 27 ? 3 : 4) : 1);
 }
 
 // Warp-specialised: warps 0..7 consume (one cell per thread), warp 8 loads and stores stages.
-template <class L, bool TRT, int K, bool EVEN, int NT, int S, bool WR>
-__global__ void __launch_bounds__(kTmaThreads, tma_min_blocks<L, K>())
+template <class L, bool TRT, int K, bool EVEN, int NT, int S, bool WR, bool PAIR = false>
+__global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR>())
     aa_tma_kernel(const __grid_constant__ StepArgs<typename Pop<K>::real> a,
                   const __grid_constant__ TmaMaps maps) {
   using P = Pop<K>;
@@ -327,16 +338,18 @@ __global__ void __launch_bounds__(kTmaThreads, tma_min_blocks<L, K>())
   // the 4096x2048 channel: no gain with FP32 populations, 8-17% slower with FP16.)
   constexpr bool whole_row = WR;
   constexpr bool bulk_out = !EVEN || WR;
+  constexpr int CW = tma_consumer_warps<PAIR>();
+  static_assert(!PAIR || (bulk_out && NT == 0), "two cells a thread: results through the stage, no tracer");
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(full + s, 1);
-      mbar_init(empty + s, kConsumerWarps);
+      mbar_init(empty + s, CW);
     }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
 
-  if (warp == kConsumerWarps) {
+  if (warp == CW) {
     // ---- producer warp. Each lane owns up to two copy jobs (job = lane, lane + 32), fixed for
     // the whole kernel and described once here: source array, row shift (even steps read slot i
     // of the row upstream of c_i), halo, element size, destination inside a stage.
@@ -529,6 +542,48 @@ __global__ void __launch_bounds__(kTmaThreads, tma_min_blocks<L, K>())
     if (lane == 0)
       for (int j = produced - S > 0 ? produced - S : 0; j < produced; ++j)
         mbar_wait(full + j % S, (unsigned)((j / S) & 1));
+    return;
+  }
+
+  if constexpr (PAIR) {
+    // ---- consumer warps, two cells a thread: cells z0 + tid and z0 + tid + T/2 of every tile.
+    constexpr int HALF = kTmaTile / 2;
+    TileWalker tw;
+    tw.init(blockIdx.x, gridDim.x, a.ny, tiles_per_row);
+    for (int j = 0; j < count; ++j, tw.next()) {
+      const int s = j % S;
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(full + s, (unsigned)((j / S) & 1)));
+      if (!ok) {
+        if (lane == 0) atomicOr(a.status, 2);
+        break;
+      }
+      const int x = tw.x, y = tw.y, z0 = tw.zt * kTmaTile;
+      unsigned char* st = stage_ptr(s);
+      float2 fv[Q];
+#pragma unroll
+      for (int i = 0; i < Q; ++i) {
+        const T* seg =
+            reinterpret_cast<const T*>(st + (size_t)(EVEN ? i : opp(i)) * St::SEG * sizeof(T));
+        const int cz = comp<L>(i, 2);
+        const int za = whole_row ? (tid - cz) & (kTmaTile - 1) : tid - cz;
+        const int zb = whole_row ? (tid + HALF - cz) & (kTmaTile - 1) : tid + HALF - cz;
+        const T va = EVEN ? seg[St::H + za] : seg[tid];
+        const T vb = EVEN ? seg[St::H + zb] : seg[tid + HALF];
+        fv[i] = make_float2(P::load_dev(&va, 0.0f), P::load_dev(&vb, 0.0f));
+      }
+      const float2 cval =
+          a.acc_mode == kAccBoussinesq
+              ? make_float2(reinterpret_cast<const Real*>(st + St::off_val)[tid],
+                            reinterpret_cast<const Real*>(st + St::off_val)[tid + HALF])
+              : make_float2(0.0f, 0.0f);
+      const int flagA = st[St::off_flag + tid], flagB = st[St::off_flag + tid + HALF];
+      const unsigned row = (unsigned)x * (unsigned)a.ny * (unsigned)a.nz + (unsigned)y * (unsigned)a.nz;
+      update_cell2<St, L, TRT, K, EVEN, kTmaTile>(a, st, tid, row + z0 + tid, row + z0 + tid + HALF,
+                                                  flagA, flagB, fv, cval);
+      fence_proxy_async();  // this thread's stage writes, visible to the bulk stores
+      __syncwarp();
+      if (lane == 0) mbar_arrive(empty + s);
+    }
     return;
   }
 
