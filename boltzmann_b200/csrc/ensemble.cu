@@ -5,10 +5,10 @@
 // (domain d owns cells [base_d, base_d + nx_d * ny_d), each domain in the reference's row-major
 // order), with one flags/rho/vel array, so one kernel launch advances every domain by one AA step.
 // A host-built tile table splits every domain row into segments of `tile` cells; a persistent
-// grid (a fixed number of CTAs per SM) walks the table, one cell per thread, with the domain's
-// sizes and relaxation rates read from a domain table. Each domain is periodic in itself (its
-// own rows wrap), exactly as a separate simulation of that size would be, and the cell update is
-// the same device function the single-domain kernels use.
+// grid (a fixed number of CTAs per SM) walks the table, two cells of a tile per thread (tile / 2
+// threads a CTA), with the domain's sizes and relaxation rates read from a domain table. Each
+// domain is periodic in itself (its own rows wrap), exactly as a separate simulation of that size
+// would be, and the cell update is the same device function the single-domain kernels use.
 //
 // Modes of lbm_ensemble_iterate:
 //   persistent        one launch per step;
@@ -57,30 +57,42 @@ __global__ void __launch_bounds__(512)
   using P = Pop<K>;
   using Real = typename P::real;
   using T = typename P::type;
+  // Two cells a thread (t and t + half of the tile): both cells' loads are issued before either
+  // update, twice the loads in flight a thread.
   for (long long t = blockIdx.x; t < e.ntiles; t += gridDim.x) {
     const TileDesc tile = e.tiles[t];
-    if ((int)threadIdx.x >= tile.len) continue;
+    const int half = (tile.len + 1) / 2;
+    if ((int)threadIdx.x >= half) continue;
     const DomainDesc dom = e.domains[tile.domain];
-    const int x = tile.x, z = tile.z0 + threadIdx.x;
-    // 2D domain on the internal (y, z) axes: rows x of the domain, cells z along a row.
-    CellPos c;
+    const int x = tile.x;
+    const bool hasB = (int)threadIdx.x + half < tile.len;
+    CellPos c[2];
     const unsigned base = (unsigned)dom.base, ny = (unsigned)dom.ny;
-    c.ox[0] = c.ox[1] = c.ox[2] = base;
-    c.oy[1] = (unsigned)x * ny;
-    c.oz[1] = (unsigned)z;
-    c.cell = base + c.oy[1] + c.oz[1];
-    if (EVEN) {
-      c.oy[0] = (unsigned)(x == 0 ? dom.nx - 1 : x - 1) * ny;
-      c.oy[2] = (unsigned)(x == dom.nx - 1 ? 0 : x + 1) * ny;
-      c.oz[0] = (unsigned)(z == 0 ? dom.ny - 1 : z - 1);
-      c.oz[2] = (unsigned)(z == dom.ny - 1 ? 0 : z + 1);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int z = tile.z0 + threadIdx.x + k * half;
+      c[k].ox[0] = c[k].ox[1] = c[k].ox[2] = base;
+      c[k].oy[1] = (unsigned)x * ny;
+      c[k].oz[1] = (unsigned)z;
+      c[k].cell = base + c[k].oy[1] + c[k].oz[1];
+      if (EVEN) {
+        c[k].oy[0] = (unsigned)(x == 0 ? dom.nx - 1 : x - 1) * ny;
+        c[k].oy[2] = (unsigned)(x == dom.nx - 1 ? 0 : x + 1) * ny;
+        c[k].oz[0] = (unsigned)(z == 0 ? dom.ny - 1 : z - 1);
+        c[k].oz[2] = (unsigned)(z == dom.ny - 1 ? 0 : z + 1);
+      }
     }
-    const int flag = a.flags[c.cell];
-    Real f[D2Q9::Q];
-    aa_load<D2Q9, P, EVEN, lbm::dev_in<K>()>(static_cast<const T*>(a.f), a.n, c, f);
+    const int flagA = a.flags[c[0].cell];
+    const int flagB = hasB ? a.flags[c[1].cell] : 1;  // a missing cell acts as a wall
+    Real fa[D2Q9::Q], fb[D2Q9::Q];
+    aa_load<D2Q9, P, EVEN, lbm::dev_in<K>()>(static_cast<const T*>(a.f), a.n, c[0], fa);
+    if (hasB) aa_load<D2Q9, P, EVEN, lbm::dev_in<K>()>(static_cast<const T*>(a.f), a.n, c[1], fb);
     Real g[1];
-    update_cell<D2Q9, TRT, K, EVEN, 0>(a, c, flag, f, g, Real(0), (Real)dom.om_pos,
+    update_cell<D2Q9, TRT, K, EVEN, 0>(a, c[0], flagA, fa, g, Real(0), (Real)dom.om_pos,
                                        (Real)dom.om_neg);
+    if (hasB)
+      update_cell<D2Q9, TRT, K, EVEN, 0>(a, c[1], flagB, fb, g, Real(0), (Real)dom.om_pos,
+                                         (Real)dom.om_neg);
   }
 }
 
@@ -90,7 +102,7 @@ struct lbm_ensemble {
   int ndomains = 0, collision = 0, storage = 0;
   std::vector<DomainDesc> domains;
   long long n = 0;                 // total cells
-  int tile = 256;                  // cells (threads) per tile
+  int tile = 256;                  // cells per tile (tile / 2 threads)
   int blocks_per_sm = 0;           // 0: occupancy limit
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -179,7 +191,7 @@ cudaError_t launch_persistent(lbm_ensemble* e, bool even, bool write_moments) {
   auto kern = even ? ensemble_step_kernel<TRT, K, true> : ensemble_step_kernel<TRT, K, false>;
   int per_sm = e->blocks_per_sm;
   if (per_sm <= 0) {
-    cudaError_t r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, e->tile, 0);
+    cudaError_t r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, e->tile / 2, 0);
     if (r != cudaSuccess) return r;
     if (per_sm < 1) per_sm = 1;
   }
@@ -187,7 +199,7 @@ cudaError_t launch_persistent(lbm_ensemble* e, bool even, bool write_moments) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
   long long grid = (long long)sms * per_sm;
   if (grid > e->ntiles) grid = e->ntiles;
-  kern<<<(unsigned)grid, e->tile, 0, e->stream>>>(a, args);
+  kern<<<(unsigned)grid, e->tile / 2, 0, e->stream>>>(a, args);
   return cudaGetLastError();
 }
 
