@@ -471,6 +471,7 @@ def run_ensemble(args) -> None:
     bpc = {"f32": 72.0, "f16": 36.0, "bf16": 36.0}[args.storage]
     peaks, peak_kind = measured_peaks()
     achieved = bpc * n * 2 * K / (graph_ms * 1e-3) / 1e9 / world  # per GPU
+    ens_traffic = profiled_traffic("ensemble_step_kernel")  # DRAM bytes per cell update (ncu)
     cpu = None if (args.no_cpu_baseline or world > 1) else cpu_ensemble_rate(setup, args.cpu_seconds)
     line = {
         "metric": "MLUPS",
@@ -506,7 +507,7 @@ def run_ensemble(args) -> None:
             "peak": peaks["hbm_gbs"],
             "unit": "GB/s",
             "frac": achieved / peaks["hbm_gbs"],
-            "traffic": None,
+            "traffic": None if ens_traffic is None else ens_traffic * setup.cells,  # a launch
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
             "algorithmic_bytes_per_cell_update": bpc,
             "kernel": "ensemble_step_kernel",
