@@ -69,3 +69,26 @@ def test_velocity_sets(d, q):
     np.testing.assert_array_equal(c[opp], -c)
     np.testing.assert_allclose((w[:, None] * c).sum(0), 0, atol=1e-15)
     assert (c[0] == 0).all()
+
+
+@pytest.mark.parametrize("name", golden_cases.names())
+def test_fixtures_regenerate_from_their_seeds(name):
+    """Each fixture's inputs come from its case's seed (its position in CASES), and, where the
+    reference's kernels are built, its outputs are exactly what they produce: the committed
+    vectors are the reference's, not a snapshot of this implementation."""
+    from oracle.oracle import reference_available
+    from tests.golden.make_golden import CASES, run_oracle, seeded_inputs
+
+    spec, inputs, outs = golden_cases.load(name)
+    assert CASES[name] == spec
+    seed = list(CASES).index(name)
+    regen = seeded_inputs(spec, seed=seed)
+    assert sorted(regen) == sorted(inputs)
+    for key, value in regen.items():
+        np.testing.assert_array_equal(value, inputs[key])
+    if not reference_available():
+        pytest.skip("reference kernels not built here")
+    for got, want in zip(run_oracle(spec, inputs, backend="reference"), outs):
+        assert sorted(got) == sorted(want)
+        for key in want:
+            np.testing.assert_array_equal(got[key], want[key])
