@@ -1,7 +1,7 @@
 """Benchmark of the lattice-Boltzmann hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload cylinder_channel|kelvin_helmholtz|taylor_green_3d|
+                    [--workload taylor_green_3d|cylinder_channel|kelvin_helmholtz|
                                 cavity_ensemble|closure|closure_forward]
                     [--storage f32|f16|bf16|f64]
 
@@ -10,9 +10,10 @@ smallest unit after which the populations are back in the reference's standard l
 The metric is MLUPS = cells x LBM steps / s, counting every cell (walls included) as the
 reference's run_sim does (python/boltzmann/simulation.py:245-246).
 
-Default workload: D2Q9 TRT cylinder channel 4096x2048 with a Boussinesq-coupled D2Q5 tracer,
-FP32 -- seeded synthetic inputs of that configuration. Its populations (302 MB + 168 MB) exceed
-the 126 MB L2, so no flush is needed between steps.
+Default workload: the D3Q27 BGK Taylor-Green vortex on 256^3 (u0 0.05, Re 1600), FP32 -- the
+largest single-GPU configuration, seeded synthetic inputs of that set-up. Its populations
+(1.81 GB) exceed the 126 MB L2, so no flush is needed between steps. Every line states the
+velocity L2 error of the benched run against an FP64 run of the same set-up and step count.
 
 ``--impl reference`` times the reference's own kernels (src/lib.cl compiled as C++, the CPU
 checker in oracle/_ref) on all host cores for the same workload, on a bounded number of steps.
@@ -74,20 +75,31 @@ def algorithmic_bytes_per_cell(setup, storage: str) -> float:
     return float(b)
 
 
-def profiled_traffic(kernel_tag: str) -> float | None:
-    """DRAM bytes per cell update from the committed ncu summary of this kernel, if any."""
+def profiled_traffic(kernel_tag: str, group: str) -> tuple[float | None, str]:
+    """DRAM bytes per cell update from the committed ncu summary of this kernel, and where the
+    figure comes from. The summary records the digest of the kernel sources it was captured
+    from; a figure whose digest differs from the sources being run is not used."""
+    from boltzmann_b200 import provenance
+
+    current = provenance.digest(group)
     for p in sorted((ROOT / "profiles").glob(f"*{kernel_tag}*.md")):
-        m = re.search(r"dram_bytes_per_cell_update:\s*([0-9.]+)", p.read_text())
-        if m:
-            return float(m.group(1))
-    return None
+        text = p.read_text()
+        m = re.search(r"dram_bytes_per_cell_update:\s*([0-9.]+)", text)
+        if not m:
+            continue
+        d = re.search(r"kernel_sources:\s*([0-9a-f]{16})", text)
+        if d is None or d.group(1) != current:
+            return None, (f"profiles/{p.name} was captured from other kernel sources "
+                          f"({d.group(1) if d else 'no digest'}, running {current}); not used")
+        return float(m.group(1)), f"ncu dram__bytes_read+write per launch, profiles/{p.name}"
+    return None, "no ncu summary for this kernel"
 
 
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
     QUERY = (
-        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
     )
@@ -96,6 +108,11 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.path = None
+        self.window: tuple[float, float] | None = None
+
+    def mark(self, t0: float, t1: float) -> None:
+        """The timed region's wall-clock window (time.time()); samples inside it are preferred."""
+        self.window = (t0, t1)
 
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -103,7 +120,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=open(self.path, "w"),
                 stderr=subprocess.DEVNULL,
             )
@@ -120,28 +137,38 @@ class ClockSampler:
     def summary(self) -> dict:
         if self.path is None or not os.path.exists(self.path):
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for line in open(self.path):
             parts = [s.strip() for s in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-            except ValueError:
+                t = time.mktime(time.strptime(parts[0].split(".")[0], "%Y/%m/%d %H:%M:%S"))
+                t += float("0." + parts[0].split(".")[1]) if "." in parts[0] else 0.0
+                rows.append((t, float(parts[2]), float(parts[3]),
+                             {n for n, v in zip(names, parts[6:10]) if v.lower() == "active"}))
+            except (ValueError, IndexError):
                 continue
-            for name, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(name)
         os.unlink(self.path)
-        if not sm:
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        where = "all samples (sampler ran around the timed region)"
+        if self.window is not None:
+            t0, t1 = self.window
+            inside = [r for r in rows if t0 - 0.025 <= r[0] <= t1 + 0.025]
+            if inside:
+                rows, where = inside, "samples inside the timed region (20 ms polling)"
+            else:  # a region shorter than the polling interval: the samples nearest to it
+                mid = 0.5 * (t0 + t1)
+                rows = sorted(rows, key=lambda r: abs(r[0] - mid))[:3]
+                where = "the 3 samples nearest the timed region (shorter than the polling)"
         return {
-            "sm_mhz": statistics.median(sm),
-            "sm_max_mhz": max(smax),
-            "reasons": sorted(reasons),
-            "samples": len(sm),
+            "sm_mhz": statistics.median(r[1] for r in rows),
+            "sm_max_mhz": max(r[2] for r in rows),
+            "reasons": sorted(set().union(*(r[3] for r in rows))),
+            "samples": len(rows),
+            "which": where,
         }
 
 
@@ -240,10 +267,19 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+WORKLOAD_TITLES = {
+    "taylor_green_3d": "D3Q27 BGK Taylor-Green vortex, u0 0.05, Re 1600",
+    "cylinder_channel": "D2Q9 TRT channel with cylinder + D2Q5 tracer + Boussinesq",
+    "kelvin_helmholtz": "D2Q9 BGK Kelvin-Helmholtz shear layer",
+}
+
+
 def config_block(setup, storage: str, world: int) -> dict:
+    from boltzmann_b200 import provenance
+
     return {
-        "workload": f"{setup.name} {'x'.join(map(str, setup.counts))}"
-        + (" + D2Q5 tracer + Boussinesq" if setup.tracers else ""),
+        "workload": f"{setup.name} {'x'.join(map(str, setup.counts))} "
+        f"({WORKLOAD_TITLES.get(setup.name, setup.name)})",
         "lattice": "D2Q9" if len(setup.counts) == 2 else "D3Q27",
         "collision": setup.collision,
         "storage": storage,
@@ -251,7 +287,21 @@ def config_block(setup, storage: str, world: int) -> dict:
         "lbm_steps_per_bench_step": 2,
         "l2": "inputs larger than L2 (populations > 126 MB); no flush",
         "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        "kernel_sources": provenance.digest("stencil"),
     }
+
+
+def velocity_l2_vs_f64(setup, vel, lbm_steps: int) -> dict:
+    """Relative velocity L2 error ||u - u64|| / ||u64|| of a run's final field against an FP64 run
+    of the same set-up on the GPU for the same number of steps (outside any timed region)."""
+    sim = build_sim(setup, "f64")
+    sim.iterate(lbm_steps)
+    _, vel64 = sim._fluid_f64()
+    del sim
+    v = np.asarray(vel, np.float64)
+    err = float(np.linalg.norm((v - vel64).ravel()) / np.linalg.norm(vel64.ravel()))
+    return {"value": err, "lbm_steps": lbm_steps, "field": "velocity",
+            "norm": "relative L2 over all cells", "against": "FP64 run on the GPU (same set-up)"}
 
 
 def run_ours(args) -> None:
@@ -275,17 +325,33 @@ def run_ours(args) -> None:
     barrier()
     torch.cuda.synchronize()
     sim._synchronize()
+    before = sim._launch_counts()
     with ClockSampler(local) as clocks:
+        t_wall0 = time.time()
         start.record(stream)
         sim._iterate_device(2 * K)
         stop.record(stream)
         stop.synchronize()
+        clocks.mark(t_wall0, time.time())
+    after = sim._launch_counts()
     barrier()
     torch.cuda.synchronize()
     elapsed_ms = max_over_ranks(start.elapsed_time(stop))
     sim.iterate(2)  # read back; checks the state is still finite
     finite = bool(np.isfinite(sim.fluid.rho).all())
+    final_vel = np.array(sim.fluid.vel, copy=True)
+    total_steps = sim.iteration
     del sim
+    # The kernels the library launched in the timed region, from its own counters.
+    direct, staged = after[0] - before[0], after[1] - before[1]
+    launches = direct + staged
+    kernel = ("aa_tma_kernel" if staged == launches else
+              "aa_step_kernel" if direct == launches else
+              f"aa_tma_kernel x{staged} + aa_step_kernel x{direct}")
+
+    l2 = None
+    if args.storage != "f64" and not args.no_l2:
+        l2 = velocity_l2_vs_f64(setup, final_vel, total_steps)
 
     lbm_steps = 2 * K
     value = world * setup.cells * lbm_steps / (elapsed_ms * 1e-3) / 1e6
@@ -295,12 +361,7 @@ def run_ours(args) -> None:
     achieved = bpc * setup.cells / (launch_ms * 1e-3) / 1e9
     tag = {"cylinder_channel": "d2q9_trt_tracer", "kelvin_helmholtz": "d2q9_bgk",
            "taylor_green_3d": "d3q27_bgk"}[args.workload] + f"_{args.storage}"
-    traffic_pc = profiled_traffic(tag)
-    # The library's own choice (csrc/aa_launch.cuh launch_one): rows of whole 256-cell tiles and
-    # at least 8 tiles per SM go through the TMA-staged kernel, everything else the direct one.
-    nz = setup.counts[-1]
-    tiles = setup.cells // 256 if nz % 256 == 0 else 0
-    kernel = "aa_tma_kernel" if nz % 256 == 0 and tiles >= 8 * 148 else "aa_step_kernel"
+    traffic_pc, traffic_src = profiled_traffic(f"{kernel}_{tag}", "stencil")
 
     # End to end through the public API with host buffers: a fresh Simulation from host arrays;
     # one iterate(2K) call uploads flags/rho/vel/C, equilibrates, steps and reads rho/vel/C back.
@@ -346,6 +407,7 @@ def run_ours(args) -> None:
                 "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"],
                 "traffic": None if traffic_pc is None else traffic_pc * setup.cells,
+                "traffic_source": traffic_src,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "algorithmic_bytes_per_cell_update": bpc,
                 "kernel": f"{kernel} ({tag})",
@@ -360,9 +422,11 @@ def run_ours(args) -> None:
                 "how": f"fresh Simulation from host arrays, one iterate({lbm_steps}) call "
                 "(upload + equilibrate + steps + read-back), host wall clock",
             },
-            "gpu_launches": lbm_steps,
+            "gpu_launches": launches,
+            "launches_by_kernel": {"aa_tma_kernel": staged, "aa_step_kernel": direct},
             "clocks": clocks.summary(),
             "finite": finite,
+            "l2_vs_f64": l2,
         }
         print(json.dumps(line), flush=True)
     group.close()
@@ -757,12 +821,14 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cylinder_channel",
+    ap.add_argument("--workload", default="taylor_green_3d",
                     choices=["cylinder_channel", "kelvin_helmholtz", "taylor_green_3d",
                              "cavity_ensemble", "closure", "closure_forward"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f64"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-l2", action="store_true",
+                    help="skip the FP64 comparison run (profiling runs only)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

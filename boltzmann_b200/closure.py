@@ -52,6 +52,7 @@ _SIGS = {
     "lbm_closure_coarsen": [_P, _P, _P, _I64, _I64, _I, _P, _P, _P, _P, _P],
     "lbm_closure_relaxation": [_P, _P, _P, _P, _P, _I64, _I64, _P, _F, _F, _F, _P, _P],
     "lbm_closure_status": [],
+    "lbm_closure_set_spin_limit": [_I64],
 }
 for _name, _args in _SIGS.items():
     getattr(_lib, _name).argtypes = _args

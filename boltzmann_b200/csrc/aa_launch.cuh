@@ -63,6 +63,9 @@ StepArgs<Real> make_step_args(const lbm_sim& s, bool write_moments) {
   a.path = s.kernel_path;
   a.omega_field = s.omega_field;
   a.status = s.status;
+  a.spin_limit = s.spin_limit < 0 ? kSpinLimit
+                                  : (unsigned)(s.spin_limit < (int64_t)kSpinLimit ? s.spin_limit
+                                                                                 : kSpinLimit);
   return a;
 }
 
@@ -183,7 +186,8 @@ cudaError_t launch_tma(const StepArgs<typename Pop<K>::real>& a, cudaStream_t st
 }
 
 template <class L, bool TRT, int K, bool EVEN, int NT>
-cudaError_t launch_one(const StepArgs<typename Pop<K>::real>& a, cudaStream_t stream) {
+cudaError_t launch_one(const StepArgs<typename Pop<K>::real>& a, cudaStream_t stream,
+                       int64_t* launches) {
   // Rows that split into whole 256-cell tiles go through the TMA-staged kernel (fused tracers:
   // none or one); everything else through the direct kernel.
   // Small domains (under ~8 tiles per SM; they sit in L2 anyway) stay on the direct kernel,
@@ -193,15 +197,21 @@ cudaError_t launch_one(const StepArgs<typename Pop<K>::real>& a, cudaStream_t st
     const bool fits = a.nz % kTmaTile == 0;
     const bool staged = a.path == 2 || (a.path == 0 && tiles >= 8LL * 148);
     if (fits && staged) {
-      if constexpr (EVEN)
-        if (a.nz == kTmaTile) return launch_tma<L, TRT, K, EVEN, NT, true>(a, stream);
-      return launch_tma<L, TRT, K, EVEN, NT, false>(a, stream);
+      cudaError_t e;
+      if (EVEN && a.nz == kTmaTile)
+        e = launch_tma<L, TRT, K, EVEN, NT, EVEN>(a, stream);
+      else
+        e = launch_tma<L, TRT, K, EVEN, NT, false>(a, stream);
+      if (e == cudaSuccess) ++launches[1];
+      return e;
     }
   }
   dim3 grid, block;
   step_geometry(a, grid, block);
   aa_step_kernel<L, TRT, K, EVEN, NT><<<grid, block, 0, stream>>>(a);
-  return cudaGetLastError();
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) ++launches[0];
+  return e;
 }
 
 template <class L, bool TRT, int K>
@@ -211,13 +221,13 @@ cudaError_t launch_typed(const lbm_sim& s, bool even, bool write_moments) {
   // Fused tracers: none, exactly one (loads hoisted with the fluid's), or a runtime count.
   const int nt = a.ntracers;
   if (even) {
-    if (nt == 0) return launch_one<L, TRT, K, true, 0>(a, s.stream);
-    if (nt == 1) return launch_one<L, TRT, K, true, 1>(a, s.stream);
-    return launch_one<L, TRT, K, true, -1>(a, s.stream);
+    if (nt == 0) return launch_one<L, TRT, K, true, 0>(a, s.stream, s.launches);
+    if (nt == 1) return launch_one<L, TRT, K, true, 1>(a, s.stream, s.launches);
+    return launch_one<L, TRT, K, true, -1>(a, s.stream, s.launches);
   }
-  if (nt == 0) return launch_one<L, TRT, K, false, 0>(a, s.stream);
-  if (nt == 1) return launch_one<L, TRT, K, false, 1>(a, s.stream);
-  return launch_one<L, TRT, K, false, -1>(a, s.stream);
+  if (nt == 0) return launch_one<L, TRT, K, false, 0>(a, s.stream, s.launches);
+  if (nt == 1) return launch_one<L, TRT, K, false, 1>(a, s.stream, s.launches);
+  return launch_one<L, TRT, K, false, -1>(a, s.stream, s.launches);
 }
 
 template <class L>

@@ -65,6 +65,7 @@ struct StepArgs {
   int path;            // kernel choice: 0 automatic, 1 direct, 2 TMA-staged (when the shape allows)
   const float* omega_field;  // per-cell om_pos (a learned closure's relaxation field), or null
   int* status;         // bit 0 set when a non-finite density or velocity is produced
+  unsigned spin_limit; // polls of a staged kernel's pipeline waits before it gives up (bit 1)
 };
 
 enum AccMode : int { kAccNone = 0, kAccConstant = 1, kAccBoussinesq = 2 };

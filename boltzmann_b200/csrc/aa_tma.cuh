@@ -58,10 +58,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
                : "memory");
 }
 
-// Bounded wait for the phase with the given parity; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+// Bounded wait for the phase with the given parity; false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity,
+                                          unsigned limit = kSpinLimit) {
   const unsigned addr = smem_u32(bar);
-  for (unsigned i = 0; i < kSpinLimit; ++i) {
+  for (unsigned i = 0; i < limit; ++i) {
     unsigned done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
@@ -493,7 +494,7 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
     tw.init(blockIdx.x, gridDim.x, a.ny, tiles_per_row);
     for (int j = 0; j < count && ok; ++j, tw.next()) {
       const int s = j % S;
-      if (j >= S) ok = mbar_wait(empty + s, (unsigned)(((j / S) - 1) & 1));
+      if (j >= S) ok = mbar_wait(empty + s, (unsigned)(((j / S) - 1) & 1), a.spin_limit);
       if (!__all_sync(0xffffffffu, ok)) break;
       if (j >= S && bulk_out) store_stage(s);
       const int x = tw.x, y = tw.y, z0 = tw.zt * kTmaTile;
@@ -531,7 +532,7 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
     // The last tiles' results (bounded waits for the consumers), then every store complete.
     if (bulk_out && ok) {
       for (int j = produced - S > 0 ? produced - S : 0; j < produced && ok; ++j) {
-        ok = __all_sync(0xffffffffu, mbar_wait(empty + j % S, (unsigned)((j / S) & 1)));
+        ok = __all_sync(0xffffffffu, mbar_wait(empty + j % S, (unsigned)((j / S) & 1), a.spin_limit));
         if (ok) store_stage(j % S);
       }
     }
@@ -552,7 +553,8 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
     tw.init(blockIdx.x, gridDim.x, a.ny, tiles_per_row);
     for (int j = 0; j < count; ++j, tw.next()) {
       const int s = j % S;
-      const bool ok = __all_sync(0xffffffffu, mbar_wait(full + s, (unsigned)((j / S) & 1)));
+      const bool ok =
+        __all_sync(0xffffffffu, mbar_wait(full + s, (unsigned)((j / S) & 1), a.spin_limit));
       if (!ok) {
         if (lane == 0) atomicOr(a.status, 2);
         break;
@@ -592,7 +594,8 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
   tw.init(blockIdx.x, gridDim.x, a.ny, tiles_per_row);
   for (int j = 0; j < count; ++j, tw.next()) {
     const int s = j % S;
-    const bool ok = __all_sync(0xffffffffu, mbar_wait(full + s, (unsigned)((j / S) & 1)));
+    const bool ok =
+        __all_sync(0xffffffffu, mbar_wait(full + s, (unsigned)((j / S) & 1), a.spin_limit));
     if (!ok) {
       if (lane == 0) atomicOr(a.status, 2);
       break;  // the producer's own waits are bounded too

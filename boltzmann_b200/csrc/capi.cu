@@ -92,8 +92,13 @@ int check_status(lbm_sim* s) {
   int word = 0;
   LBM_CUDA(cudaMemcpyAsync(&word, s->status, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   LBM_CUDA(cudaStreamSynchronize(s->stream));
-  if (word & 2)
+  if (word & 2) {
+    // Reported once: the bit is cleared so that the simulation can be restored and run again.
+    const int rest = word & ~2;
+    LBM_CUDA(cudaMemcpyAsync(s->status, &rest, sizeof(int), cudaMemcpyHostToDevice, s->stream));
+    LBM_CUDA(cudaStreamSynchronize(s->stream));
     return fail(LBM_ERR_CUDA, "an AA step gave up waiting for its staged copies (status bit 1)");
+  }
   return LBM_OK;
 }
 
@@ -436,6 +441,19 @@ int lbm_set_kernel_path(lbm_sim* sim, int path) {
   if (path < LBM_PATH_AUTO || path > LBM_PATH_STAGED)
     return fail(LBM_ERR_ARGUMENT, "unknown kernel path");
   sim->kernel_path = path;
+  return LBM_OK;
+}
+
+int lbm_set_spin_limit(lbm_sim* sim, int64_t polls) {
+  if (int rc = activate(sim)) return rc;
+  sim->spin_limit = polls < 0 ? -1 : polls;
+  return LBM_OK;
+}
+
+int lbm_launch_counts(lbm_sim* sim, int64_t* direct, int64_t* staged) {
+  if (int rc = activate(sim)) return rc;
+  if (direct) *direct = sim->launches[0];
+  if (staged) *staged = sim->launches[1];
   return LBM_OK;
 }
 

@@ -858,10 +858,15 @@ __device__ __forceinline__ void cl_mbar_init(uint64_t* bar, unsigned count) {
                : "memory");
 }
 
-// Bounded wait for the phase with the given parity; false on timeout.
-__device__ __forceinline__ bool cl_mbar_wait(uint64_t* bar, unsigned parity) {
+// Polls of the fused kernel's wait for its tensor-core products before it gives up
+// (lbm_closure_set_spin_limit); the wait that drains MMAs still in flight keeps the default.
+__device__ unsigned g_closure_spin_limit = kClosureSpinLimit;
+
+// Bounded wait for the phase with the given parity; false after `limit` polls.
+__device__ __forceinline__ bool cl_mbar_wait(uint64_t* bar, unsigned parity,
+                                             unsigned limit = kClosureSpinLimit) {
   const unsigned addr = smem_addr(bar);
-  for (unsigned i = 0; i < kClosureSpinLimit; ++i) {
+  for (unsigned i = 0; i < limit; ++i) {
     unsigned done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
@@ -985,6 +990,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   const uint32_t idesc = umma_idesc_bf16(128, 32);
   const unsigned a1c_addr = smem_addr(a1c), w2c_addr = smem_addr(w2c);
   bool healthy = true;
+  const unsigned spin_limit = g_closure_spin_limit;
   // Layer-1 A fragments: element e of k-step kk holds input k = 16 kk + 2 tq + 8 (e >> 1), that
   // is tap k / 4 and the channel pair (k & 3) / 2 of the feature cell shifted by the tap. The
   // offset of that word from the cell's own (in 32-bit words of the feature region) depends on
@@ -1151,7 +1157,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       umma_commit(mma_done);
     }
     if (t + (int)gridDim.x < ntiles) stage_features(t + gridDim.x);
-    const bool got = cl_mbar_wait(mma_done, phase);
+    const bool got = cl_mbar_wait(mma_done, phase, spin_limit);
     phase ^= 1u;
     if (!__syncthreads_and(got)) {
       healthy = false;
@@ -1556,6 +1562,13 @@ int lbm_closure_relaxation(const float* params, const uint16_t* params_bf16, con
   const int grid = (int)std::min<int64_t>(ntiles, (int64_t)device_sms());
   closure_fused_kernel<<<grid, kFusedThreads, kFusedSmem, (cudaStream_t)stream>>>(fa);
   CL_CUDA(cudaGetLastError());
+  return LBM_OK;
+}
+
+int lbm_closure_set_spin_limit(int64_t polls) {
+  const unsigned v = polls < 0 ? kClosureSpinLimit
+                               : (unsigned)std::min<int64_t>(polls, (int64_t)kClosureSpinLimit);
+  CL_CUDA(cudaMemcpyToSymbol(g_closure_spin_limit, &v, sizeof(unsigned)));
   return LBM_OK;
 }
 

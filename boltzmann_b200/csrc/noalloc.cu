@@ -15,16 +15,20 @@
 // In host code `g_partials` names a host-side stand-in, not device memory: handing it to a kernel
 // would fault, or, where the GPU can reach host memory, silently use the wrong memory. The device
 // address is obtained once per device with cudaGetSymbolAddress (with that device current) on the
-// first call there; make that first call before any stream capture begins.
+// first call there; make that first call before any stream capture begins. The address belongs to
+// the device's context: when that context is destroyed and created again (cudaDeviceReset), the
+// next call notices the new context (its unique id, cuCtxGetId) and looks the address up again.
 //
 // Every call on a device shares g_partials and it keeps the last call's contents. Each call
 // overwrites every slot it later reads (nothing needs to start at zero), but two calls whose
 // kernels overlap on the GPU (different streams, no ordering between them) race on the array.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
 #include <mutex>
 #include <string>
+#include <utility>
 
 #include "../../include/lbm_cuda.h"
 #include "lattice.cuh"
@@ -123,8 +127,34 @@ __global__ void __launch_bounds__(kThreads)
 
 std::mutex g_setup_mutex;
 void* g_scratch_address[kMaxDevices] = {};
+unsigned long long g_scratch_context[kMaxDevices] = {};
 
-// Device address of g_partials for the current device, looked up once per device.
+// Unique id of the calling thread's current context (cuCtxGetId, through the runtime's driver
+// entry points: no link against libcuda), or 0 when it cannot be read.
+unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static const auto fns = [] {
+    void *cur = nullptr, *id = nullptr;
+    cudaDriverEntryPointQueryResult q1{}, q2{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &cur, cudaEnableDefault, &q1) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess)
+      cur = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &id, cudaEnableDefault, &q2) != cudaSuccess ||
+        q2 != cudaDriverEntryPointSuccess)
+      id = nullptr;
+    return std::make_pair(reinterpret_cast<GetCurrent>(cur), reinterpret_cast<GetId>(id));
+  }();
+  if (fns.first == nullptr || fns.second == nullptr) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long ident = 0;
+  if (fns.first(&ctx) != CUDA_SUCCESS || ctx == nullptr) return 0;
+  if (fns.second(ctx, &ident) != CUDA_SUCCESS) return 0;
+  return ident;
+}
+
+// Device address of g_partials for the current device: looked up once per device, and again
+// when the device's context has been re-created since.
 int scratch_address(double (**out)[4]) {
   int device = 0;
   cudaError_t e = cudaGetDevice(&device);
@@ -136,8 +166,10 @@ int scratch_address(double (**out)[4]) {
     lbm::set_last_error("device index out of range");
     return LBM_ERR_ARGUMENT;
   }
+  // 0 when this thread has no current context yet (the look-up below binds the primary one).
+  const unsigned long long ctx = current_context_id();
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (g_scratch_address[device] == nullptr) {
+  if (g_scratch_address[device] == nullptr || ctx == 0 || g_scratch_context[device] != ctx) {
     void* ptr = nullptr;
     e = cudaGetSymbolAddress(&ptr, g_partials);
     if (e != cudaSuccess || ptr == nullptr) {
@@ -145,6 +177,7 @@ int scratch_address(double (**out)[4]) {
       return LBM_ERR_CUDA;
     }
     g_scratch_address[device] = ptr;
+    g_scratch_context[device] = current_context_id();
   }
   *out = static_cast<double (*)[4]>(g_scratch_address[device]);
   return LBM_OK;

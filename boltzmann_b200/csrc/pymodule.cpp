@@ -560,6 +560,13 @@ PYBIND11_MODULE(boltzmann, m) {
                st.iteration += (uint64_t)every;
              }
            })
+      .def("_launch_counts",
+           [](const Simulation& s) {
+             // AA step launches so far: (direct kernel, TMA-staged kernel).
+             int64_t direct = 0, staged = 0;
+             check(lbm_launch_counts(s.st->h, &direct, &staged));
+             return py::make_tuple(direct, staged);
+           })
       .def("_synchronize", [](const Simulation& s) { check(lbm_synchronize(s.st->h)); })
       .def("_stream", [](const Simulation& s) {
         void* p = nullptr;

@@ -29,6 +29,9 @@ struct lbm_sim {
   int device = 0;
   cudaStream_t stream = nullptr;
   int kernel_path = 0;  // LBM_PATH_AUTO / _DIRECT / _STAGED
+  int64_t spin_limit = -1;  // polls of the staged kernel's pipeline waits; < 0: the default
+  // AA step launches since creation, per kernel variant: [0] direct, [1] TMA-staged.
+  mutable int64_t launches[2] = {0, 0};
   const float* omega_field = nullptr;  // caller-owned per-cell om_pos, or null
 
   void* f = nullptr;    // [q][N] populations in the storage type

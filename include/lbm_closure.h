@@ -123,6 +123,13 @@ LBM_API int lbm_closure_relaxation(const float* params, const uint16_t* params_b
                                    int64_t nx, int64_t ny, const float* norm, float tau0,
                                    float gain, float max_dtau, float* omega, void* stream);
 
+/* Polls that the lbm_closure_relaxation kernel makes, on the current device, while waiting for
+ * its tensor-core products before it gives up (polls < 0: the default, 2^22). A kernel that gives
+ * up records it for lbm_closure_status, still waits (with the default bound) for the products in
+ * flight, frees its tensor memory and returns; 0 makes the wait give up at once, a way to exercise
+ * that path. Synchronous. No reference counterpart. */
+LBM_API int lbm_closure_set_spin_limit(int64_t polls);
+
 /* LBM_OK, or LBM_ERR_STATE when a lbm_closure_relaxation kernel on the current device gave up
  * waiting for its tensor-core products (bounded wait) since the last call; its omega is then
  * incomplete. Synchronous; clears the condition. */

@@ -152,6 +152,20 @@ LBM_API int lbm_nonfinite(lbm_sim* sim, int* out);
  * counterpart. */
 LBM_API int lbm_set_kernel_path(lbm_sim* sim, int path);
 
+/* Polls that each pipeline wait of the TMA-staged kernel makes before it gives up (the copies of
+ * a stage, or its release by the consumer warps); polls < 0 restores the default (2^22). A kernel
+ * that gives up sets bit 1 of the status word, still waits (with the default bound) for the
+ * copies it issued, and returns; the next synchronising call (lbm_download_fluid,
+ * lbm_synchronize) then fails with LBM_ERR_CUDA, once, and the populations are not valid until
+ * they are uploaded again. 0 makes every pipeline wait give up at once: a way to exercise that
+ * path. No reference counterpart. */
+LBM_API int lbm_set_spin_limit(lbm_sim* sim, int64_t polls);
+
+/* AA step launches since lbm_create, per kernel variant: the direct kernel (aa_step_kernel) and
+ * the TMA-staged one (aa_tma_kernel). Host-side counters, no synchronisation. No reference
+ * counterpart (instrumentation: which kernel a workload actually ran). */
+LBM_API int lbm_launch_counts(lbm_sim* sim, int64_t* direct, int64_t* staged);
+
 /* Per-cell relaxation rate: `field` is a device array of N floats (omega+ of every cell) that
  * the caller owns and keeps alive, written on the simulation's stream (a learned closure's output);
  * NULL returns to the uniform rate. Fixed cells still relax with 1; the force shift keeps the
@@ -178,8 +192,10 @@ LBM_API int lbm_stream(lbm_sim* sim, void** stream);
  *   stream cudaStream_t to run on (NULL: the default stream). Asynchronous.
  * Scratch is a fixed 64 KiB per device inside this library, held until the process exits, so n is
  * limited to 134,217,728 cells (LBM_ERR_ARGUMENT beyond). The first call on a device looks up that
- * scratch's address; make it before any stream capture. All calls share the scratch: calls that
- * may overlap on the GPU (unordered streams) race. */
+ * scratch's address; make it before any stream capture. After the device's context is created
+ * again (cudaDeviceReset) the next call looks the address up again, so make that call outside
+ * stream capture too. All calls share the scratch: calls that may overlap on the GPU (unordered
+ * streams) race. */
 LBM_API int lbm_population_sums_noalloc(int dim, int q, int storage, const void* f, int64_t n,
                                         double* out, void* stream);
 

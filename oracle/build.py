@@ -4,8 +4,8 @@
 * ``oracle/_ref/liblbm_ref.so`` -- the reference's own kernels (``src/lib.cl`` of
   djbarker/boltzmann, unmodified, plus the D3Q27 TRT kernel its generator writes) compiled as
   C++ behind ``ref_shim.h`` with the host loop of ``ref_driver.cpp``. Built only where the
-  reference tree exists (``BOLTZMANN_REFERENCE``, default ``/root/reference``); elsewhere the
-  prebuilt library is used as it is.
+  reference tree exists (``BOLTZMANN_REFERENCE``, else a ``reference`` directory beside this
+  repository's root); elsewhere the prebuilt library is used as it is.
 
 Both are checkers for the CUDA product and its CPU baseline; nothing in the product imports them.
 """
@@ -28,7 +28,9 @@ CFLAGS = ["-O3", "-march=x86-64-v3", "-fPIC", "-shared", "-fopenmp", "-ffp-contr
 
 
 def reference_root() -> Path:
-    return Path(os.environ.get("BOLTZMANN_REFERENCE", "/root/reference"))
+    """The reference checkout: $BOLTZMANN_REFERENCE, else ``../reference`` from the repo root."""
+    env = os.environ.get("BOLTZMANN_REFERENCE")
+    return Path(env) if env else HERE.parent.parent / "reference"
 
 
 def _run(cmd: list[str]) -> None:

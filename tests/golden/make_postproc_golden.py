@@ -12,7 +12,11 @@ from pathlib import Path
 
 import numpy as np
 
-REFERENCE_PYTHON = Path("/root/reference/python")
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+from oracle.build import reference_root  # noqa: E402
+
+REFERENCE_PYTHON = reference_root() / "python"
 OUT = Path(__file__).resolve().parent / "postproc.npz"
 
 

@@ -1,7 +1,10 @@
 """The reference's Python API on the CUDA backend.
 
 The first four tests are the hot-path tests of the reference's own suite
-(python/tests/test_core.py:57-127), with "cpu" meaning "the CUDA device" as everywhere here.
+(python/tests/test_core.py:57-127), with "cpu" meaning "the CUDA device" as everywhere here,
+imported as the reference's scripts import them: ``boltzmann.core`` through the aliases of
+``boltzmann_b200.alias``. (The reference's module itself runs unchanged through the same aliases
+in ``tests/test_reference_suite_cpu.py`` wherever the reference checkout exists.)
 """
 
 from __future__ import annotations
@@ -11,9 +14,12 @@ import tempfile
 import numpy as np
 import pytest
 
-from boltzmann_b200.core import PanicException, Simulation, bgk, trt
-from tests import golden_cases
-from tests.golden_cases import rel_err
+from boltzmann_b200 import alias
+
+alias.install()
+from boltzmann.core import PanicException, Simulation, bgk, trt  # noqa: E402
+from tests import golden_cases  # noqa: E402
+from tests.golden_cases import rel_err  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
