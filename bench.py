@@ -49,16 +49,20 @@ def measured_peaks() -> tuple[dict, str]:
     return PEAKS_FALLBACK, "fallback"
 
 
-def make_setup(workload: str):
+def make_setup(workload: str, size: int | None = None):
+    """The workload's set-up; ``size`` (profiling captures only) shrinks the Taylor-Green box to
+    size^3 cells or the channel to 2 size x size."""
     from boltzmann_b200 import workloads
 
     if workload in ("cylinder_channel", "closure"):
         # closure: the reference's way to that accuracy is the plain fine channel itself
+        if size:
+            return workloads.cylinder_channel(2 * size, size, radius=size / 32)
         return workloads.cylinder_channel()
     if workload == "kelvin_helmholtz":
         return workloads.kelvin_helmholtz()
     if workload == "taylor_green_3d":
-        return workloads.taylor_green_3d()
+        return workloads.taylor_green_3d(size or 256)
     raise SystemExit(f"unknown workload {workload}")
 
 
@@ -241,7 +245,7 @@ def run_reference(args) -> None:
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    setup = make_setup(args.workload)
+    setup = make_setup(args.workload, args.size)
     # Bounded: the whole arm stays within a few minutes.
     base = cpu_reference_rate(setup, budget_s=min(60.0, 2.0 * max(args.steps, 1)),
                               max_pairs=args.steps)
@@ -314,7 +318,7 @@ def run_ours(args) -> None:
     group = Group()  # replicas: no data-path collective; barrier + max of device times only
     barrier, max_over_ranks = group.barrier, group.max
 
-    setup = make_setup(args.workload)
+    setup = make_setup(args.workload, args.size)
     K, W = args.steps, max(args.warmup, 3)
 
     # Device-timed run: inputs resident in HBM, only the AA kernels in the timed region.
@@ -365,19 +369,21 @@ def run_ours(args) -> None:
 
     # End to end through the public API with host buffers: a fresh Simulation from host arrays;
     # one iterate(2K) call uploads flags/rho/vel/C, equilibrates, steps and reads rho/vel/C back.
-    sim2 = build_sim(setup, args.storage)
-    barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    sim2.iterate(lbm_steps)
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
     n = setup.cells
     d = len(setup.counts)
     nt = len(setup.tracers)
     h2d = n * (1 + d) * 4 + n * 4 + nt * n * 4  # flags (sent as i32), rho, vel, tracer C
     d2h = n * (1 + d) * 4 + nt * n * 4
-    e2e_value = world * n * lbm_steps / e2e_s / 1e6
-    del sim2
+    e2e_value = None
+    if not args.no_e2e:
+        sim2 = build_sim(setup, args.storage)
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim2.iterate(lbm_steps)
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        e2e_value = world * n * lbm_steps / e2e_s / 1e6
+        del sim2
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -414,7 +420,7 @@ def run_ours(args) -> None:
                 "frac_of_nominal_8tbs": achieved / 8000.0,
             },
             "cpu_baseline": cpu,
-            "e2e": {
+            "e2e": None if e2e_value is None else {
                 "value": e2e_value,
                 "unit": "MLUPS",
                 "h2d_bytes_per_step": h2d / K,
@@ -829,6 +835,11 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-l2", action="store_true",
                     help="skip the FP64 comparison run (profiling runs only)")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="skip the end-to-end run (profiling runs only)")
+    ap.add_argument("--size", type=int, default=None,
+                    help="smaller box for profiling captures: Taylor-Green size^3, channel "
+                    "2 size x size")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

