@@ -51,7 +51,8 @@ def measured_peaks() -> tuple[dict, str]:
 
 def make_setup(workload: str, size: int | None = None):
     """The workload's set-up; ``size`` (profiling captures only) shrinks the Taylor-Green box to
-    size^3 cells or the channel to 2 size x size."""
+    size x size x 256 cells (rows stay one 256-cell tile, as at full size, so the same kernel
+    runs) or the channel to 2 size x size."""
     from boltzmann_b200 import workloads
 
     if workload in ("cylinder_channel", "closure"):
@@ -62,7 +63,7 @@ def make_setup(workload: str, size: int | None = None):
     if workload == "kelvin_helmholtz":
         return workloads.kelvin_helmholtz()
     if workload == "taylor_green_3d":
-        return workloads.taylor_green_3d(size or 256)
+        return workloads.taylor_green_3d(size, nz=256) if size else workloads.taylor_green_3d()
     raise SystemExit(f"unknown workload {workload}")
 
 
@@ -838,8 +839,8 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end run (profiling runs only)")
     ap.add_argument("--size", type=int, default=None,
-                    help="smaller box for profiling captures: Taylor-Green size^3, channel "
-                    "2 size x size")
+                    help="smaller box for profiling captures: Taylor-Green size x size x 256, "
+                    "channel 2 size x size")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

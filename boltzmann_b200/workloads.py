@@ -123,26 +123,29 @@ def cylinder_channel(
     )
 
 
-def taylor_green_3d(n: int = 256, u0: float = 0.05, re: float = 1600.0) -> Setup:
+def taylor_green_3d(n: int = 256, u0: float = 0.05, re: float = 1600.0,
+                    nz: int | None = None) -> Setup:
     """u = u0 (sin kx cos ky cos kz, -cos kx sin ky cos kz, 0), k = 2 pi / n, with the pressure
     field in rho = 1 + 3 p, p = u0^2/16 (cos 2kx + cos 2ky)(cos 2kz + 2);
-    nu = u0 (n / 2 pi) / re, tau = 3 nu + 1/2."""
-    k = 2 * math.pi / n
+    nu = u0 (n / 2 pi) / re, tau = 3 nu + 1/2. ``nz`` (profiling cases only) stretches the box
+    along z to n x n x nz, with k_z = 2 pi / nz."""
+    nz = nz or n
+    k, kz = 2 * math.pi / n, 2 * math.pi / nz
     c = np.arange(n, dtype=np.float64)
-    X, Y, Z = np.meshgrid(c, c, c, indexing="ij")
-    vel = np.empty((n, n, n, 3), np.float32)
-    vel[..., 0] = u0 * np.sin(k * X) * np.cos(k * Y) * np.cos(k * Z)
-    vel[..., 1] = -u0 * np.cos(k * X) * np.sin(k * Y) * np.cos(k * Z)
+    X, Y, Z = np.meshgrid(c, c, np.arange(nz, dtype=np.float64), indexing="ij")
+    vel = np.empty((n, n, nz, 3), np.float32)
+    vel[..., 0] = u0 * np.sin(k * X) * np.cos(k * Y) * np.cos(kz * Z)
+    vel[..., 1] = -u0 * np.cos(k * X) * np.sin(k * Y) * np.cos(kz * Z)
     vel[..., 2] = 0.0
-    p = u0**2 / 16 * (np.cos(2 * k * X) + np.cos(2 * k * Y)) * (np.cos(2 * k * Z) + 2)
+    p = u0**2 / 16 * (np.cos(2 * k * X) + np.cos(2 * k * Y)) * (np.cos(2 * kz * Z) + 2)
     rho = (1.0 + 3.0 * p).astype(np.float32)
     nu = u0 * (n / (2 * math.pi)) / re
     return Setup(
         "taylor_green_3d",
-        [n, n, n],
+        [n, n, nz],
         "bgk",
         3 * nu + 0.5,
-        np.zeros((n, n, n), np.int32),
+        np.zeros((n, n, nz), np.int32),
         rho,
         vel,
         params={"u0": u0, "re": re, "nu": nu},

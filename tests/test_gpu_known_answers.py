@@ -148,7 +148,7 @@ def test_3d_body_force_reaches_every_row():
     from tests.capi import CApiSim
 
     counts = [3, 10, 4]  # ny = 10 > nz = 4
-    g = np.array([1e-4, 2e-4, 3e-4], np.float32)
+    g = np.array([1e-3, 2e-3, 3e-3], np.float32)  # velocities well above FP32 rounding noise
     om = OOmega.bgk(0.7)
     sim = CApiSim(counts, om.kind, float(om.pos))
     sim.set_gravity(g)
@@ -158,7 +158,7 @@ def test_3d_body_force_reaches_every_row():
     ref.iterate(2)
     # This backend: a uniform shift of every cell.
     assert np.ptp(sim.vel.reshape(-1, 3), axis=0).max() < 1e-9
-    assert (np.abs(sim.vel[..., 2]) > 1e-4).all()
+    assert (np.abs(sim.vel[..., 2]) > 1e-3).all()
     # Rows 1 .. nz-2 agree with the reference kernels.
     inner = slice(1, counts[2] - 1)
     assert rel_err(sim.vel[:, inner], ref.vel[:, inner]) < 1e-5
