@@ -162,7 +162,8 @@ def test_3d_body_force_reaches_every_row():
     # Rows 1 .. nz-2 agree with the reference kernels.
     inner = slice(1, counts[2] - 1)
     assert rel_err(sim.vel[:, inner], ref.vel[:, inner]) < 1e-5
-    # Rows nz+1 .. ny-2 stay at rest in the reference.
+    # Rows nz+1 .. ny-2 stay at rest in the reference (up to FP32 residue of ~1e-8) and move
+    # here like every other row.
     beyond = slice(counts[2] + 1, counts[1] - 1)
-    assert np.abs(ref.vel[:, beyond]).max() == 0.0
-    assert np.abs(sim.vel[:, beyond]).min() > 0.0
+    assert np.abs(ref.vel[:, beyond]).max() < 1e-6
+    assert (np.abs(sim.vel[:, beyond, :, 2]) > 1e-3).all()
