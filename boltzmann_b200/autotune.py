@@ -1,4 +1,5 @@
-"""Autotuner for the ensemble's launch shape (tile width and CTAs per SM).
+"""Autotuner for the ensemble's launch shape: the kernel (row-staged, or tiles of a given width)
+and its CTAs per SM.
 
 Candidates are timed on the ensemble itself with CUDA events on its stream (a few AA step pairs
 each, after one warm-up pair); the populations are saved before and restored after, so tuning
@@ -17,8 +18,11 @@ from pathlib import Path
 
 import numpy as np
 
-TILES = (32, 64, 128, 256, 512)
+TILES = (32, 64, 128, 256, 512)  # tile kernel widths
 BLOCKS = (0, 2, 4, 8)
+ROW_BLOCKS = (0, 1, 2)  # CTAs per SM of the row-staged kernel (tile 0; 0 = as many as fit)
+ROW_MAX = 512  # longest row the row-staged kernel takes
+KERNELS = "rows+tiles"  # part of the cache key: entries made before the row kernel are ignored
 
 
 def cache_path() -> Path:
@@ -34,7 +38,8 @@ def size_class(ens) -> str:
 
 def key(ens, storage: str) -> str:
     coll = "trt" if ens.collision else "bgk"
-    return f"D2Q9/{coll}/{storage}/{size_class(ens)}"
+    rows = "rows" if max(b for _, b in ens.counts) <= ROW_MAX else "tiles-only"
+    return f"D2Q9/{coll}/{storage}/{size_class(ens)}/{KERNELS}/{rows}"
 
 
 def _load() -> dict:
@@ -84,9 +89,10 @@ def tune(ens, storage: str = "f32", use_cache: bool = True, pairs: int = 4) -> d
     saved = ens.populations()
     saved_iteration = ens.iteration
     timings = {}
-    for tile in TILES:
-        for blocks in BLOCKS:
-            timings[f"{tile}x{blocks}"] = time_shape(ens, tile, blocks, pairs)
+    shapes = [(0, b) for b in ROW_BLOCKS] if max(b for _, b in ens.counts) <= ROW_MAX else []
+    shapes += [(t, b) for t in TILES for b in BLOCKS]
+    for tile, blocks in shapes:
+        timings[f"{tile}x{blocks}"] = time_shape(ens, tile, blocks, pairs)
     best = min(timings, key=timings.get)
     tile, blocks = (int(v) for v in best.split("x"))
     ens.set_shape(tile, blocks)

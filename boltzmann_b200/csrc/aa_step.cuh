@@ -80,6 +80,17 @@ __host__ __device__ constexpr int comp(int i, int a) {
     return a == 0 ? 0 : L::c(i, a - 1);
 }
 
+// comp<L>(i, A) for a slot index known only at run time (a producer lane's job), selected from
+// the compile-time entries so that the velocity table is never materialised in local memory.
+template <class L, int A>
+__device__ __forceinline__ int comp_rt(int i) {
+  int v = 0;
+#pragma unroll
+  for (int k = 0; k < L::Q; ++k)
+    if (k == i) v = comp<L>(k, A);
+  return v;
+}
+
 // Upstream coordinate along one axis for a velocity component cc (coordinate - cc, wrapped).
 __device__ __forceinline__ int upstream_coord(int cc, int minus1, int same, int plus1) {
   return cc > 0 ? minus1 : (cc < 0 ? plus1 : same);

@@ -380,11 +380,11 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
       Job jb{nullptr, 0, 0, 0, 0, 1, 0u, 0, false};
       if (op < Q) {
         const int slot = op;  // stage position op holds slot op (odd steps read opp(i) from it)
-        const int cz = EVEN && !whole_row ? comp<L>(op, 2) : 0;
+        const int cz = EVEN && !whole_row ? comp_rt<L, 2>(op) : 0;
         jb.base = reinterpret_cast<const unsigned char*>(static_cast<const T*>(a.f) +
                                                          (size_t)slot * a.n);
-        jb.cx = EVEN ? comp<L>(op, 0) : 0;
-        jb.cy = EVEN ? comp<L>(op, 1) : 0;
+        jb.cx = EVEN ? comp_rt<L, 0>(op) : 0;
+        jb.cy = EVEN ? comp_rt<L, 1>(op) : 0;
         jb.hl = cz > 0 ? St::H : 0;
         jb.hr = cz < 0 ? St::H : 0;
         jb.es = sizeof(T);
@@ -395,10 +395,10 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
         if constexpr (NT == 1) {
           const int i = op - Q;
           const int slot = i;
-          const int cz = EVEN && !whole_row ? comp<TL>(i, 2) : 0;
+          const int cz = EVEN && !whole_row ? comp_rt<TL, 2>(i) : 0;
           jb.base = reinterpret_cast<const unsigned char*>(a.tr[0].g + (size_t)slot * a.n);
-          jb.cx = EVEN ? comp<TL>(i, 0) : 0;
-          jb.cy = EVEN ? comp<TL>(i, 1) : 0;
+          jb.cx = EVEN ? comp_rt<TL, 0>(i) : 0;
+          jb.cy = EVEN ? comp_rt<TL, 1>(i) : 0;
           jb.hl = cz > 0 ? St::HG : 0;
           jb.hr = cz < 0 ? St::HG : 0;
           jb.es = sizeof(Real);
@@ -438,8 +438,8 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
 #pragma unroll
       for (int m = 0; m < 4; ++m) {
         const int slot = 4 * lane + m < Q ? 4 * lane + m : Q - 1;
-        gcx[m] = comp<L>(slot, 0);
-        gcy[m] = comp<L>(slot, 1);
+        gcx[m] = comp_rt<L, 0>(slot);
+        gcy[m] = comp_rt<L, 1>(slot);
       }
     }
     auto group_rows = [&](int x, int y, int (&r)[4]) {

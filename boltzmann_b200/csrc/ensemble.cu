@@ -10,6 +10,18 @@
 // domain is periodic in itself (its own rows wrap), exactly as a separate simulation of that size
 // would be, and the cell update is the same device function the single-domain kernels use.
 //
+// Two kernels walk the domains:
+//   rows (default whenever every row has at most 512 cells): one domain row per work item. A
+//     producer warp copies, with one TMA bulk copy per population slot, the 16-byte-aligned
+//     superset of the row that slot is read from (on even steps rows x-1, x, x+1 of the domain,
+//     wrapped; on odd steps row x) plus the row's flags into a ring of shared-memory stages,
+//     completing on the stage's mbarrier; four consumer warps collide from shared memory (the
+//     periodic z-wrap is an index wrap in the stage) and store the results with coalesced
+//     per-thread stores. The loads of several rows stay in flight while others are computed, so
+//     no thread waits on HBM latency.
+//   tiles: row segments of `tile` cells, two cells per thread, loads straight into registers
+//     (lbm_ensemble_set_shape with a tile width; the only kernel for rows over 512 cells).
+//
 // Modes of lbm_ensemble_iterate:
 //   persistent        one launch per step;
 //   persistent+graph  the same launches captured once into a CUDA graph of `chunk` step pairs and
@@ -26,6 +38,7 @@
 
 #include "../../include/lbm_cuda.h"
 #include "aa_step.cuh"
+#include "aa_tma.cuh"
 #include "sim.h"
 
 namespace {
@@ -96,13 +109,210 @@ __global__ void __launch_bounds__(512)
   }
 }
 
+// ---- The row-staged kernel.
+
+constexpr int kRowMax = 512;               // longest domain row the staged kernel takes
+constexpr int kRowConsumerWarps = 4;       // 128 threads: up to four cells each per row
+constexpr int kRowThreads = 32 * kRowConsumerWarps + 32;  // + the producer warp
+
+struct RowDesc {
+  int domain;
+  int x;  // row of the domain (the reference's x)
+};
+
+struct RowArgs {
+  const DomainDesc* domains;
+  const RowDesc* rows;
+  long long nrows;
+};
+
+// Written by the producer into each stage next to the copies: where the row's cells are and
+// where each copied segment starts inside its stage slot.
+struct RowHead {
+  unsigned row[3];        // first cell of rows x-1, x, x+1 of the domain (wrapped)
+  int ny;                 // cells in the row
+  float om_pos, om_neg;   // the domain's relaxation rates
+  unsigned char off[10];  // slots 0-8 and the flags: element offset of the row in its segment
+};
+
+template <int K>
+struct RowStage {
+  using T = typename lbm::Pop<K>::type;
+  static constexpr int kSlack = 16 / (int)sizeof(T);  // elements before a 16-byte boundary
+  static constexpr int SEG = kRowMax + kSlack;         // elements per slot segment
+  static constexpr size_t seg_bytes = (size_t)SEG * sizeof(T);
+  static_assert(seg_bytes % 16 == 0, "slot segments start on 16-byte boundaries");
+  static constexpr size_t off_flags = 9 * seg_bytes;
+  static constexpr size_t off_head = off_flags + kRowMax + 16;
+  static constexpr size_t bytes = (off_head + sizeof(RowHead) + 127) / 128 * 128;
+  // Ring depth: about 58 KB of stages a CTA for 32-bit populations (three CTAs a SM), 40 KB for
+  // 16-bit ones (five).
+  static constexpr int stages = sizeof(T) == 4 ? 3 : 4;
+};
+
+// Slots whose velocity has a positive / negative component along internal axis 1 (the
+// reference's x), as bit masks: a runtime slot index then needs no table in local memory.
+__host__ __device__ constexpr unsigned row_shift_mask(int sign) {
+  unsigned m = 0;
+  for (int i = 0; i < lbm::D2Q9::Q; ++i)
+    if (lbm::comp<lbm::D2Q9>(i, 1) * sign > 0) m |= 1u << i;
+  return m;
+}
+
+template <int K>
+constexpr size_t row_smem_bytes() {
+  return RowStage<K>::stages * RowStage<K>::bytes + 2 * RowStage<K>::stages * sizeof(uint64_t);
+}
+
+template <bool TRT, int K, bool EVEN>
+__global__ void __launch_bounds__(kRowThreads)
+    ensemble_rows_kernel(const __grid_constant__ lbm::StepArgs<typename lbm::Pop<K>::real> a,
+                         const RowArgs e) {
+  using namespace lbm;
+  using P = Pop<K>;
+  using Real = typename P::real;
+  using T = typename P::type;
+  using St = RowStage<K>;
+  constexpr int S = St::stages;
+  constexpr int CW = kRowConsumerWarps;
+
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)S * St::bytes);
+  uint64_t* empty = full + S;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // This CTA's rows: blockIdx.x + j * gridDim.x, j = 0 .. count-1.
+  const int count =
+      (long long)blockIdx.x < e.nrows ? (int)((e.nrows - 1 - blockIdx.x) / gridDim.x + 1) : 0;
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, CW);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+
+  if (warp == CW) {
+    // ---- producer warp: lane k < 9 copies slot k, lane 9 the flags.
+    bool ok = true;
+    int produced = 0;
+    for (int j = 0; j < count && ok; ++j) {
+      const int s = j % S;
+      if (j >= S) ok = mbar_wait(empty + s, (unsigned)(((j / S) - 1) & 1), a.spin_limit);
+      if (!__all_sync(0xffffffffu, ok)) {
+        ok = false;
+        break;
+      }
+      const long long r = blockIdx.x + (long long)j * gridDim.x;
+      const RowDesc rd = e.rows[r];
+      const DomainDesc dom = e.domains[rd.domain];
+      const unsigned ny = (unsigned)dom.ny;
+      const unsigned rowx = (unsigned)dom.base + (unsigned)rd.x * ny;
+      const unsigned rowm = (unsigned)dom.base + (unsigned)(rd.x == 0 ? dom.nx - 1 : rd.x - 1) * ny;
+      const unsigned rowp = (unsigned)dom.base + (unsigned)(rd.x == dom.nx - 1 ? 0 : rd.x + 1) * ny;
+      unsigned char* st = smem + (size_t)s * St::bytes;
+      uintptr_t lo = 0, addr = 0;
+      unsigned bytes = 0, dst = 0;
+      int es = 1;
+      if (lane < 9) {
+        // Even steps read slot i of the row upstream of c_i (internal axis 1: the reference's
+        // x); odd steps read the row itself.
+        constexpr unsigned kPlus = row_shift_mask(1), kMinus = row_shift_mask(-1);
+        const unsigned row = !EVEN ? rowx
+                                   : (((kPlus >> lane) & 1u) ? rowm
+                                                             : (((kMinus >> lane) & 1u) ? rowp : rowx));
+        addr = reinterpret_cast<uintptr_t>(static_cast<const T*>(a.f) + (size_t)lane * a.n + row);
+        es = (int)sizeof(T);
+        dst = (unsigned)(lane * St::seg_bytes);
+      } else if (lane == 9) {
+        addr = reinterpret_cast<uintptr_t>(a.flags + rowx);
+        dst = (unsigned)St::off_flags;
+      }
+      if (lane < 10) {
+        // The 16-byte-aligned superset of the row's ny elements (at most ny + 16 bytes: it fits
+        // the segment, and the arrays are padded so that it stays inside their allocations).
+        lo = addr & ~(uintptr_t)15;
+        const uintptr_t hi = (addr + (uintptr_t)ny * es + 15) & ~(uintptr_t)15;
+        bytes = (unsigned)(hi - lo);
+      }
+      const unsigned expect = __reduce_add_sync(0xffffffffu, bytes);
+      RowHead* h = reinterpret_cast<RowHead*>(st + St::off_head);
+      if (lane < 10) h->off[lane] = (unsigned char)((addr - lo) / (uintptr_t)es);
+      if (lane == 0) {
+        h->row[0] = rowm;
+        h->row[1] = rowx;
+        h->row[2] = rowp;
+        h->ny = (int)ny;
+        h->om_pos = dom.om_pos;
+        h->om_neg = dom.om_neg;
+      }
+      __syncwarp();
+      if (lane == 0) mbar_expect_tx(full + s, expect);  // releases the header writes too
+      __syncwarp();
+      if (bytes) bulk_copy(st + dst, reinterpret_cast<const void*>(lo), bytes, full + s);
+      produced = j + 1;
+    }
+    if (!ok && lane == 0) atomicOr(a.status, 2);
+    // Leave only once the copies of the last stages have landed (bounded), so that no copy
+    // writes into shared memory after the CTA is gone.
+    if (lane == 0)
+      for (int j = produced - S > 0 ? produced - S : 0; j < produced; ++j)
+        mbar_wait(full + j % S, (unsigned)((j / S) & 1));
+    return;
+  }
+
+  // ---- consumer warps: thread tid updates cells tid, tid + 128, ... of every row.
+  for (int j = 0; j < count; ++j) {
+    const int s = j % S;
+    const bool ok =
+        __all_sync(0xffffffffu, mbar_wait(full + s, (unsigned)((j / S) & 1), a.spin_limit));
+    if (!ok) {
+      if (lane == 0) atomicOr(a.status, 2);
+      break;  // the producer's own waits are bounded too
+    }
+    const unsigned char* st = smem + (size_t)s * St::bytes;
+    const RowHead& h = *reinterpret_cast<const RowHead*>(st + St::off_head);
+    const int ny = h.ny;
+    for (int z = tid; z < ny; z += 32 * CW) {
+      CellPos c;
+      c.ox[0] = c.ox[1] = c.ox[2] = 0u;
+      c.oy[0] = h.row[0];
+      c.oy[1] = h.row[1];
+      c.oy[2] = h.row[2];
+      c.oz[0] = (unsigned)(z == 0 ? ny - 1 : z - 1);
+      c.oz[1] = (unsigned)z;
+      c.oz[2] = (unsigned)(z == ny - 1 ? 0 : z + 1);
+      c.cell = h.row[1] + (unsigned)z;
+      const int flag = st[St::off_flags + h.off[9] + z];
+      Real fv[D2Q9::Q];
+#pragma unroll
+      for (int i = 0; i < D2Q9::Q; ++i) {
+        const int slot = EVEN ? i : opp(i);
+        const T* seg = reinterpret_cast<const T*>(st + (size_t)slot * St::seg_bytes) + h.off[slot];
+        // even: the upstream cell's z is z - c_iz, wrapped
+        const int cz = comp<D2Q9>(i, 2);
+        const unsigned zi = !EVEN ? (unsigned)z : (cz > 0 ? c.oz[0] : (cz < 0 ? c.oz[2] : c.oz[1]));
+        if constexpr (dev_in<K>())
+          fv[i] = P::load_dev(seg + zi, weight<D2Q9, Real>(i));
+        else
+          fv[i] = P::load(seg + zi, weight<D2Q9, Real>(i));
+      }
+      Real g[1];
+      update_cell<D2Q9, TRT, K, EVEN, 0>(a, c, flag, fv, g, Real(0), (Real)h.om_pos,
+                                         (Real)h.om_neg);
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(empty + s);  // this warp is done with stage s
+  }
+}
+
 }  // namespace
 
 struct lbm_ensemble {
   int ndomains = 0, collision = 0, storage = 0;
   std::vector<DomainDesc> domains;
   long long n = 0;                 // total cells
-  int tile = 256;                  // cells per tile (tile / 2 threads)
+  int tile = 0;                    // cells per tile (tile / 2 threads); 0: the row-staged kernel
   int blocks_per_sm = 0;           // 0: occupancy limit
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -110,7 +320,10 @@ struct lbm_ensemble {
   DomainDesc* d_domains = nullptr;
   TileDesc* d_tiles = nullptr;
   long long ntiles = 0;
-  int tiles_for = 0;               // tile width the table was built for
+  int tiles_for = -1;              // tile width the table was built for
+  RowDesc* d_rows = nullptr;       // the row table of the row-staged kernel (tile == 0)
+  long long nrows = 0;
+  int max_row = 0;                 // longest row (cells)
   // Captured graph of `graph_pairs` step pairs in persistent mode.
   cudaGraphExec_t graph = nullptr;
   int graph_pairs = 0, graph_tile = 0, graph_blocks = 0;
@@ -147,9 +360,24 @@ void drop_graph(lbm_ensemble* e) {
   e->graph_pairs = 0;
 }
 
-// (Re)builds the tile table for the current tile width.
+// (Re)builds the tile table for the current tile width, or the row table (tile == 0).
 int build_tiles(lbm_ensemble* e) {
-  if (e->d_tiles && e->tiles_for == e->tile) return LBM_OK;
+  if (e->tiles_for == e->tile) return LBM_OK;
+  if (e->tile == 0) {
+    if (e->d_rows == nullptr) {
+      std::vector<RowDesc> rows;
+      for (int d = 0; d < e->ndomains; ++d)
+        for (int x = 0; x < e->domains[d].nx; ++x) rows.push_back(RowDesc{d, x});
+      ENS_CUDA(cudaMalloc((void**)&e->d_rows, rows.size() * sizeof(RowDesc)));
+      ENS_CUDA(cudaMemcpyAsync(e->d_rows, rows.data(), rows.size() * sizeof(RowDesc),
+                               cudaMemcpyHostToDevice, e->stream));
+      ENS_CUDA(cudaStreamSynchronize(e->stream));
+      e->nrows = (long long)rows.size();
+    }
+    e->tiles_for = 0;
+    drop_graph(e);
+    return LBM_OK;
+  }
   std::vector<TileDesc> tiles;
   for (int d = 0; d < e->ndomains; ++d) {
     const DomainDesc& dom = e->domains[d];
@@ -203,6 +431,34 @@ cudaError_t launch_persistent(lbm_ensemble* e, bool even, bool write_moments) {
   return cudaGetLastError();
 }
 
+template <bool TRT, int K, bool EVEN>
+cudaError_t launch_rows_parity(lbm_ensemble* e, bool write_moments) {
+  using Real = typename lbm::Pop<K>::real;
+  auto kern = ensemble_rows_kernel<TRT, K, EVEN>;
+  constexpr size_t smem = row_smem_bytes<K>();
+  static std::once_flag once;
+  static cudaError_t setup_err = cudaSuccess;
+  static int occupancy = 1;
+  std::call_once(once, [&] {
+    setup_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (setup_err == cudaSuccess)
+      setup_err =
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy, kern, kRowThreads, smem);
+    if (occupancy < 1) occupancy = 1;
+  });
+  if (setup_err != cudaSuccess) return setup_err;
+  const int per_sm = e->blocks_per_sm > 0 ? std::min(e->blocks_per_sm, occupancy) : occupancy;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
+  long long grid = (long long)sms * per_sm;
+  if (grid > e->nrows) grid = e->nrows;
+  lbm::StepArgs<Real> a = base_args<Real>(e, write_moments);
+  a.spin_limit = lbm::kSpinLimit;
+  kern<<<(unsigned)grid, kRowThreads, smem, e->stream>>>(a, RowArgs{e->d_domains, e->d_rows,
+                                                                    e->nrows});
+  return cudaGetLastError();
+}
+
 template <bool TRT, int K>
 cudaError_t launch_per_domain(lbm_ensemble* e, bool even, bool write_moments) {
   using Real = typename lbm::Pop<K>::real;
@@ -234,6 +490,9 @@ cudaError_t launch_per_domain(lbm_ensemble* e, bool even, bool write_moments) {
 template <bool TRT, int K>
 cudaError_t launch_step(lbm_ensemble* e, bool even, bool write_moments, int mode) {
   if (mode == 2) return launch_per_domain<TRT, K>(e, even, write_moments);
+  if (e->tile == 0)
+    return even ? launch_rows_parity<TRT, K, true>(e, write_moments)
+                : launch_rows_parity<TRT, K, false>(e, write_moments);
   return launch_persistent<TRT, K>(e, even, write_moments);
 }
 
@@ -290,6 +549,7 @@ void release(lbm_ensemble* e) {
   cudaFree(e->shell.status);
   cudaFree(e->d_domains);
   cudaFree(e->d_tiles);
+  cudaFree(e->d_rows);
   if (e->stream) cudaStreamDestroy(e->stream);
 }
 
@@ -322,6 +582,7 @@ int lbm_ensemble_create(int ndomains, const int64_t* counts, int collision,
     }
     DomainDesc dom{n, (int)nx, (int)ny, omega_pos[d], omega_neg ? omega_neg[d] : 0.0f};
     e->domains.push_back(dom);
+    e->max_row = std::max(e->max_row, (int)ny);
     n += nx * ny;
   }
   if (n >= ((long long)1 << 32)) {
@@ -348,8 +609,12 @@ int lbm_ensemble_create(int ndomains, const int64_t* counts, int collision,
   s.n = n;
   s.device = e->device;
   s.stream = e->stream;
+  // Rows longer than the staged kernel's stages go through the tile kernel.
+  e->tile = e->max_row <= kRowMax ? 0 : 256;
   const size_t flag_bytes = ((size_t)n + 255) / 256 * 256;
-  if ((r = cudaMalloc(&s.f, (size_t)n * 9 * lbm::pop_bytes(storage))) != cudaSuccess ||
+  // 256 bytes of padding after the populations: the staged kernel's aligned row copies may
+  // reach up to 15 bytes past the last slot's last row.
+  if ((r = cudaMalloc(&s.f, (size_t)n * 9 * lbm::pop_bytes(storage) + 256)) != cudaSuccess ||
       (r = cudaMalloc(&s.rho, (size_t)n * sizeof(float))) != cudaSuccess ||
       (r = cudaMalloc(&s.vel, (size_t)n * 2 * sizeof(float))) != cudaSuccess ||
       (r = cudaMalloc((void**)&s.flags, flag_bytes)) != cudaSuccess ||
@@ -389,8 +654,10 @@ int lbm_ensemble_cells(lbm_ensemble* e, int64_t* total) {
 
 int lbm_ensemble_set_shape(lbm_ensemble* e, int tile_cells, int blocks_per_sm) {
   if (int rc = activate(e)) return rc;
-  if (tile_cells < 32 || tile_cells > 512 || tile_cells % 32 != 0)
-    return efail(LBM_ERR_ARGUMENT, "tile_cells must be a multiple of 32 in [32, 512]");
+  if (tile_cells != 0 && (tile_cells < 32 || tile_cells > 512 || tile_cells % 32 != 0))
+    return efail(LBM_ERR_ARGUMENT, "tile_cells must be 0 or a multiple of 32 in [32, 512]");
+  if (tile_cells == 0 && e->max_row > kRowMax)
+    return efail(LBM_ERR_UNSUPPORTED, "the row-staged kernel takes rows of at most 512 cells");
   if (blocks_per_sm < 0 || blocks_per_sm > 64)
     return efail(LBM_ERR_ARGUMENT, "blocks_per_sm must be in [0, 64]");
   e->tile = tile_cells;

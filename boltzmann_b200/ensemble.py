@@ -61,7 +61,9 @@ class Ensemble:
         self.rho = np.ones(self.n, np.float32)
         self.vel = np.zeros((self.n, 2), np.float32)
         self.iteration = 0
-        self.shape = (256, 0)
+        # The library's default: the row-staged kernel (tile 0) when every row has at most 512
+        # cells, else tiles of 256 cells; CTAs per SM as many as fit.
+        self.shape = (0 if max(b for _, b in self.counts) <= 512 else 256, 0)
 
     def __del__(self):
         if getattr(self, "h", None):

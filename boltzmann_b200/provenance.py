@@ -17,7 +17,8 @@ CSRC = Path(__file__).resolve().parent / "csrc"
 GROUPS = {
     "stencil": ["aa_step.cuh", "aa_tma.cuh", "aa_pair.cuh", "aa_launch.cuh", "lattice.cuh",
                 "storage.cuh", "aa_d2q9.cu", "aa_d3q27.cu"],
-    "ensemble": ["ensemble.cu", "aa_step.cuh", "lattice.cuh", "storage.cuh"],
+    "ensemble": ["ensemble.cu", "aa_step.cuh", "aa_tma.cuh", "aa_pair.cuh", "lattice.cuh",
+                 "storage.cuh"],
     "closure": ["closure.cu"],
 }
 

@@ -218,8 +218,12 @@ LBM_API int lbm_ensemble_create(int ndomains, const int64_t* counts, int collisi
                                 lbm_ensemble** out);
 LBM_API int lbm_ensemble_destroy(lbm_ensemble* ens);
 LBM_API int lbm_ensemble_cells(lbm_ensemble* ens, int64_t* total);
-/* Tile shape: cells (threads) per tile, a multiple of 32 in [32, 512], and CTAs per SM of the
- * persistent grid (0 = occupancy limit). Chosen by the autotuner (boltzmann_b200.autotune). */
+/* Launch shape of the persistent kernel. tile_cells 0 selects the row-staged kernel (the default
+ * when every domain row has at most 512 cells; LBM_ERR_UNSUPPORTED otherwise): one domain row
+ * per work item, loaded by TMA bulk copies into a shared-memory ring. A multiple of 32 in
+ * [32, 512] selects the tile kernel with that many cells per tile (two per thread), loads straight
+ * into registers. blocks_per_sm: CTAs per SM of the persistent grid (0 = as many as fit).
+ * Chosen by the autotuner (boltzmann_b200.autotune); every shape gives the same bits. */
 LBM_API int lbm_ensemble_set_shape(lbm_ensemble* ens, int tile_cells, int blocks_per_sm);
 LBM_API int lbm_ensemble_upload(lbm_ensemble* ens, const int32_t* flags, const float* rho,
                                 const float* vel);

@@ -36,14 +36,47 @@ def test_modes_agree_bitwise(mode):
     np.testing.assert_array_equal(ens.populations(), ref.populations())
 
 
-@pytest.mark.parametrize("tile,blocks", [(32, 0), (64, 4), (512, 1)])
-def test_shapes_agree_bitwise(tile, blocks):
-    _, ref = _small_ensemble()
+@pytest.mark.parametrize("tile,blocks", [(0, 1), (32, 0), (64, 4), (512, 1)])
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_shapes_agree_bitwise(tile, blocks, storage):
+    """The row-staged kernel (tile 0, the default) and the tile kernel of every width give the
+    same bits: the same cell update on the same inputs, only the data movement differs."""
+    _, ref = _small_ensemble(storage)
+    ref.set_shape(64, 0)
     ref.iterate(40)
-    _, ens = _small_ensemble()
+    _, ens = _small_ensemble(storage)
     ens.set_shape(tile, blocks)
     ens.iterate(40)
     np.testing.assert_array_equal(ens.populations(), ref.populations())
+    np.testing.assert_array_equal(ens.rho, ref.rho)
+
+
+def test_row_kernel_takes_rows_up_to_512_cells():
+    """Rows of 512 cells (the row-staged kernel's longest) and 513 (tile kernel only) next to
+    short ones; each domain still equals its single-domain run."""
+    from boltzmann_b200.ensemble import Ensemble
+    from tests.capi import CApiSim
+
+    counts = [(6, 512), (5, 37), (3, 16)]
+    taus = [0.6, 0.7, 0.55]
+    rng = np.random.default_rng(3)
+    ens = Ensemble(counts, tau=taus)
+    assert ens.shape[0] == 0  # row-staged by default
+    n = sum(a * b for a, b in counts)
+    ens.rho[...] = (1 + rng.uniform(-0.01, 0.01, n)).astype(np.float32)
+    ens.vel[...] = rng.uniform(-0.05, 0.05, (n, 2)).astype(np.float32)
+    rho0, vel0 = ens.rho.copy(), ens.vel.copy()
+    ens.iterate(20)
+    start = 0
+    for (a, b), tau in zip(counts, taus):
+        single = CApiSim([a, b], 0, float(np.float32(1.0 / tau)))
+        single.rho[...] = rho0[start:start + a * b].reshape(a, b)
+        single.vel[...] = vel0[start:start + a * b].reshape(a, b, 2)
+        single.iterate(20)
+        np.testing.assert_array_equal(ens.rho[start:start + a * b].reshape(a, b), single.rho)
+        start += a * b
+    wide = Ensemble([(4, 513), (3, 20)], tau=[0.6, 0.6])
+    assert wide.shape[0] != 0  # rows over 512 cells: the tile kernel
 
 
 def test_domains_equal_single_simulations():
