@@ -181,4 +181,7 @@ def test_autotune_cache_key():
         n = 64 * 64 + 128 * 128 + 512 * 512
         collision = 0
 
-    assert autotune.key(Fake(), "f32") == "D2Q9/bgk/f32/cells2^18-width2^7"
+    assert autotune.key(Fake(), "f32") == "D2Q9/bgk/f32/cells2^18-width2^7/rows+tiles/rows"
+    Fake.counts = [(64, 64), (600, 600)]  # a row over 512 cells: tile kernels only
+    Fake.n = 64 * 64 + 600 * 600
+    assert autotune.key(Fake(), "f32").endswith("/tiles-only")
