@@ -490,7 +490,7 @@ def run_ensemble(args) -> None:
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     group = Group()
-    full = workloads.lid_driven_cavities()
+    full = workloads.lid_driven_cavities(count=args.size or 512)
     # The domains are independent: under torchrun each rank advances its own share (by cells).
     setup = full if world == 1 else full.subset(shard_by_cells(full.counts, world)[rank])
     K, W = args.steps, max(args.warmup, 3)
@@ -504,7 +504,12 @@ def run_ensemble(args) -> None:
 
     ens = fresh()
     ens.iterate(2 * W, mode="persistent")
-    tuned = autotune.tune(ens, args.storage, use_cache=True, pairs=2)
+    if args.shape:
+        tile, blocks = (int(v) for v in args.shape.split(","))
+        ens.set_shape(tile, blocks)
+        tuned = {"tile": tile, "blocks_per_sm": blocks, "cached": False, "fixed": True}
+    else:
+        tuned = autotune.tune(ens, args.storage, use_cache=True, pairs=2)
     stream = torch.cuda.ExternalStream(ens.stream())
 
     def timed(mode: str, pairs: int) -> float:
@@ -565,6 +570,7 @@ def run_ensemble(args) -> None:
         "data": "synthetic",
         "config": {
             "workload": f"lid_driven_cavities x{len(full.counts)} (sides 64..512, Re 100..5000)",
+            "ensemble_cells": setup.cells,
             "parallelism": "single GPU" if world == 1 else
             f"{world} ranks, domains sharded by cell count (no collective)",
             "lattice": "D2Q9",
@@ -576,7 +582,8 @@ def run_ensemble(args) -> None:
             "kernel_sources": __import__("boltzmann_b200.provenance").provenance.digest("ensemble"),
             "tile_cells": tuned["tile"],
             "blocks_per_sm": tuned["blocks_per_sm"],
-            "autotune": "cached" if tuned.get("cached") else "searched",
+            "autotune": "fixed by --shape" if tuned.get("fixed") else
+            ("cached" if tuned.get("cached") else "searched"),
             "autotune_ms_per_pair": tuned.get("timings_ms_per_pair"),
             "l2": "inputs larger than L2; no flush",
         },
@@ -848,8 +855,11 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end run (profiling runs only)")
     ap.add_argument("--size", type=int, default=None,
-                    help="smaller box for profiling captures: Taylor-Green size x size x 256, "
-                    "channel 2 size x size")
+                    help="smaller case for profiling captures: Taylor-Green size x size x 256, "
+                    "channel 2 size x size, ensemble the first `size` cavities")
+    ap.add_argument("--shape", default=None,
+                    help="ensemble only: fixed launch shape 'tile,blocks_per_sm' instead of the "
+                    "autotuner's (tile 0: the row-staged kernel)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
