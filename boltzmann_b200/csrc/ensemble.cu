@@ -145,9 +145,10 @@ struct RowStage {
   static constexpr size_t off_flags = 9 * seg_bytes;
   static constexpr size_t off_head = off_flags + kRowMax + 16;
   static constexpr size_t bytes = (off_head + sizeof(RowHead) + 127) / 128 * 128;
-  // Ring depth: about 58 KB of stages a CTA for 32-bit populations (three CTAs a SM), 40 KB for
-  // 16-bit ones (five).
-  static constexpr int stages = sizeof(T) == 4 ? 3 : 4;
+  // Ring depth: two stages (38 KB) a CTA for 32-bit populations and three (30 KB) for 16-bit
+  // ones, so that five to seven CTAs share an SM: the consumers' cell updates, not the loads,
+  // need the warps.
+  static constexpr int stages = sizeof(T) == 4 ? 2 : 3;
 };
 
 // Slots whose velocity has a positive / negative component along internal axis 1 (the
@@ -271,35 +272,42 @@ __global__ void __launch_bounds__(kRowThreads)
       break;  // the producer's own waits are bounded too
     }
     const unsigned char* st = smem + (size_t)s * St::bytes;
+    // The row's header into registers once (the cell loop's global stores could otherwise alias
+    // it, as far as the compiler knows, and force a reload per cell).
     const RowHead& h = *reinterpret_cast<const RowHead*>(st + St::off_head);
     const int ny = h.ny;
+    const unsigned row0 = h.row[0], row1 = h.row[1], row2 = h.row[2];
+    const Real om_p = (Real)h.om_pos, om_n = (Real)h.om_neg;
+    const T* seg[D2Q9::Q];
+#pragma unroll
+    for (int i = 0; i < D2Q9::Q; ++i)
+      seg[i] = reinterpret_cast<const T*>(st + (size_t)i * St::seg_bytes) + h.off[i];
+    const unsigned char* fl = st + St::off_flags + h.off[9];
     for (int z = tid; z < ny; z += 32 * CW) {
       CellPos c;
       c.ox[0] = c.ox[1] = c.ox[2] = 0u;
-      c.oy[0] = h.row[0];
-      c.oy[1] = h.row[1];
-      c.oy[2] = h.row[2];
+      c.oy[0] = row0;
+      c.oy[1] = row1;
+      c.oy[2] = row2;
       c.oz[0] = (unsigned)(z == 0 ? ny - 1 : z - 1);
       c.oz[1] = (unsigned)z;
       c.oz[2] = (unsigned)(z == ny - 1 ? 0 : z + 1);
-      c.cell = h.row[1] + (unsigned)z;
-      const int flag = st[St::off_flags + h.off[9] + z];
+      c.cell = row1 + (unsigned)z;
+      const int flag = fl[z];
       Real fv[D2Q9::Q];
 #pragma unroll
       for (int i = 0; i < D2Q9::Q; ++i) {
         const int slot = EVEN ? i : opp(i);
-        const T* seg = reinterpret_cast<const T*>(st + (size_t)slot * St::seg_bytes) + h.off[slot];
         // even: the upstream cell's z is z - c_iz, wrapped
         const int cz = comp<D2Q9>(i, 2);
         const unsigned zi = !EVEN ? (unsigned)z : (cz > 0 ? c.oz[0] : (cz < 0 ? c.oz[2] : c.oz[1]));
         if constexpr (dev_in<K>())
-          fv[i] = P::load_dev(seg + zi, weight<D2Q9, Real>(i));
+          fv[i] = P::load_dev(seg[slot] + zi, weight<D2Q9, Real>(i));
         else
-          fv[i] = P::load(seg + zi, weight<D2Q9, Real>(i));
+          fv[i] = P::load(seg[slot] + zi, weight<D2Q9, Real>(i));
       }
       Real g[1];
-      update_cell<D2Q9, TRT, K, EVEN, 0>(a, c, flag, fv, g, Real(0), (Real)h.om_pos,
-                                         (Real)h.om_neg);
+      update_cell<D2Q9, TRT, K, EVEN, 0>(a, c, flag, fv, g, Real(0), om_p, om_n);
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(empty + s);  // this warp is done with stage s
