@@ -283,42 +283,31 @@ __global__ void __launch_bounds__(kRowThreads)
     for (int i = 0; i < D2Q9::Q; ++i)
       seg[i] = reinterpret_cast<const T*>(st + (size_t)i * St::seg_bytes) + h.off[i];
     const unsigned char* fl = st + St::off_flags + h.off[9];
-    // Two cells a thread per pass (z and z + 128): both cells' operands are read before either
-    // update, so two independent cell updates interleave.
-    constexpr int W = 32 * CW;
-    for (int z0 = tid; z0 < ny; z0 += 2 * W) {
-      CellPos c[2];
-      int flag[2];
-      Real fv[2][D2Q9::Q];
+    for (int z = tid; z < ny; z += 32 * CW) {
+      CellPos c;
+      c.ox[0] = c.ox[1] = c.ox[2] = 0u;
+      c.oy[0] = row0;
+      c.oy[1] = row1;
+      c.oy[2] = row2;
+      c.oz[0] = (unsigned)(z == 0 ? ny - 1 : z - 1);
+      c.oz[1] = (unsigned)z;
+      c.oz[2] = (unsigned)(z == ny - 1 ? 0 : z + 1);
+      c.cell = row1 + (unsigned)z;
+      const int flag = fl[z];
+      Real fv[D2Q9::Q];
 #pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const int z = z0 + k * W < ny ? z0 + k * W : z0;  // a missing second cell repeats the first
-        c[k].ox[0] = c[k].ox[1] = c[k].ox[2] = 0u;
-        c[k].oy[0] = row0;
-        c[k].oy[1] = row1;
-        c[k].oy[2] = row2;
-        c[k].oz[0] = (unsigned)(z == 0 ? ny - 1 : z - 1);
-        c[k].oz[1] = (unsigned)z;
-        c[k].oz[2] = (unsigned)(z == ny - 1 ? 0 : z + 1);
-        c[k].cell = row1 + (unsigned)z;
-        flag[k] = fl[z];
-#pragma unroll
-        for (int i = 0; i < D2Q9::Q; ++i) {
-          const int slot = EVEN ? i : opp(i);
-          // even: the upstream cell's z is z - c_iz, wrapped
-          const int cz = comp<D2Q9>(i, 2);
-          const unsigned zi =
-              !EVEN ? (unsigned)z : (cz > 0 ? c[k].oz[0] : (cz < 0 ? c[k].oz[2] : c[k].oz[1]));
-          if constexpr (dev_in<K>())
-            fv[k][i] = P::load_dev(seg[slot] + zi, weight<D2Q9, Real>(i));
-          else
-            fv[k][i] = P::load(seg[slot] + zi, weight<D2Q9, Real>(i));
-        }
+      for (int i = 0; i < D2Q9::Q; ++i) {
+        const int slot = EVEN ? i : opp(i);
+        // even: the upstream cell's z is z - c_iz, wrapped
+        const int cz = comp<D2Q9>(i, 2);
+        const unsigned zi = !EVEN ? (unsigned)z : (cz > 0 ? c.oz[0] : (cz < 0 ? c.oz[2] : c.oz[1]));
+        if constexpr (dev_in<K>())
+          fv[i] = P::load_dev(seg[slot] + zi, weight<D2Q9, Real>(i));
+        else
+          fv[i] = P::load(seg[slot] + zi, weight<D2Q9, Real>(i));
       }
       Real g[1];
-      update_cell<D2Q9, TRT, K, EVEN, 0>(a, c[0], flag[0], fv[0], g, Real(0), om_p, om_n);
-      if (z0 + W < ny)
-        update_cell<D2Q9, TRT, K, EVEN, 0>(a, c[1], flag[1], fv[1], g, Real(0), om_p, om_n);
+      update_cell<D2Q9, TRT, K, EVEN, 0>(a, c, flag, fv, g, Real(0), om_p, om_n);
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(empty + s);  // this warp is done with stage s
