@@ -16,11 +16,9 @@
 //     superset of the row that slot is read from (on even steps rows x-1, x, x+1 of the domain,
 //     wrapped; on odd steps row x) plus the row's flags into a ring of shared-memory stages,
 //     completing on the stage's mbarrier; four consumer warps collide from shared memory (the
-//     periodic z-wrap is an index wrap in the stage) and write every result back into the stage
-//     position it was read from; before refilling a stage the producer writes each slot's row
-//     back with one bulk store of its 16-byte-aligned interior plus plain stores of the few
-//     elements on either side. The loads of several rows stay in flight while others are
-//     computed, so no thread waits on HBM latency.
+//     periodic z-wrap is an index wrap in the stage) and store the results with coalesced
+//     per-thread stores. The loads of several rows stay in flight while others are computed, so
+//     no thread waits on HBM latency.
 //   tiles: row segments of `tile` cells, two cells per thread, loads straight into registers
 //     (lbm_ensemble_set_shape with a tile width; the only kernel for rows over 512 cells).
 //
@@ -167,35 +165,6 @@ constexpr size_t row_smem_bytes() {
   return RowStage<K>::stages * RowStage<K>::bytes + 2 * RowStage<K>::stages * sizeof(uint64_t);
 }
 
-// update_cell's output into the stage: every population goes to the stage position it was read
-// from (slot i at the cell itself on odd steps; slot i of the upstream cell, shifted and wrapped,
-// on even steps). Each slot segment then holds the whole new row of that slot, which the producer
-// writes back.
-template <int K>
-struct RowStageSink {
-  using T = typename lbm::Pop<K>::type;
-  T* seg[lbm::D2Q9::Q];  // slot segments, already advanced to the row's first element
-
-  template <class L, class P, bool EVEN, bool DEV>
-  __device__ __forceinline__ void fluid(typename P::type*, long long, const lbm::CellPos& c,
-                                        const typename P::real (&v)[L::Q]) const {
-    using Real = typename P::real;
-#pragma unroll
-    for (int i = 0; i < L::Q; ++i) {
-      const int cz = lbm::comp<L>(i, 2);
-      const unsigned p = !EVEN ? c.oz[1] : (cz > 0 ? c.oz[0] : (cz < 0 ? c.oz[2] : c.oz[1]));
-      const Real val = EVEN ? v[lbm::opp(i)] : v[i];
-      if constexpr (DEV)
-        P::store_dev(seg[i] + p, val, lbm::weight<L, Real>(i));
-      else
-        P::store(seg[i] + p, val, lbm::weight<L, Real>(i));
-    }
-  }
-  template <class TT, class TP, bool EVEN>
-  __device__ __forceinline__ void tracer(typename TP::type*, long long, const lbm::CellPos&,
-                                         const typename TP::real (&)[TT::Q]) const {}
-};
-
 template <bool TRT, int K, bool EVEN>
 __global__ void __launch_bounds__(kRowThreads)
     ensemble_rows_kernel(const __grid_constant__ lbm::StepArgs<typename lbm::Pop<K>::real> a,
@@ -226,47 +195,6 @@ __global__ void __launch_bounds__(kRowThreads)
 
   if (warp == CW) {
     // ---- producer warp: lane k < 9 copies slot k, lane 9 the flags.
-    constexpr unsigned kPlus = row_shift_mask(1), kMinus = row_shift_mask(-1);
-    constexpr int kSlack = St::kSlack;
-    // Writes a consumed stage back: per slot, the 16-byte-aligned interior of the row with one
-    // bulk store (lane = slot), the few elements before and after it with plain stores.
-    auto store_stage = [&](int s) {
-      unsigned char* st = smem + (size_t)s * St::bytes;
-      const RowHead& h = *reinterpret_cast<const RowHead*>(st + St::off_head);
-      const int ny = h.ny;
-      // first cell of the row slot i belongs to (the row it was read from)
-      auto slot_row = [&](int i) {
-        return !EVEN ? h.row[1]
-                     : (((kPlus >> i) & 1u) ? h.row[0] : (((kMinus >> i) & 1u) ? h.row[2] : h.row[1]));
-      };
-      auto interior = [&](int i, int& lo, int& hi) {
-        lo = (kSlack - h.off[i]) % kSlack;
-        if (lo > ny) lo = ny;
-        hi = lo + (ny - lo) / kSlack * kSlack;
-      };
-      if (lane < D2Q9::Q) {
-        int lo, hi;
-        interior(lane, lo, hi);
-        if (hi > lo) {
-          T* g = static_cast<T*>(a.f) + (size_t)lane * a.n + slot_row(lane) + lo;
-          const unsigned char* src = st + (size_t)lane * St::seg_bytes + (size_t)(h.off[lane] + lo) * sizeof(T);
-          bulk_store(g, src, (unsigned)((hi - lo) * (int)sizeof(T)));
-        }
-      }
-      for (int e = lane; e < D2Q9::Q * 2 * kSlack; e += 32) {
-        const int i = e / (2 * kSlack), k = e - i * 2 * kSlack;
-        int lo, hi;
-        interior(i, lo, hi);
-        const int p = k < kSlack ? k : hi + (k - kSlack);
-        if (k < kSlack ? p < lo : p < ny) {
-          const T* src = reinterpret_cast<const T*>(st + (size_t)i * St::seg_bytes) + h.off[i] + p;
-          static_cast<T*>(a.f)[(size_t)i * a.n + slot_row(i) + p] = *src;
-        }
-      }
-      bulk_commit();
-      bulk_wait_read();
-      __syncwarp();
-    };
     bool ok = true;
     int produced = 0;
     for (int j = 0; j < count && ok; ++j) {
@@ -276,7 +204,6 @@ __global__ void __launch_bounds__(kRowThreads)
         ok = false;
         break;
       }
-      if (j >= S) store_stage(s);
       const long long r = blockIdx.x + (long long)j * gridDim.x;
       const RowDesc rd = e.rows[r];
       const DomainDesc dom = e.domains[rd.domain];
@@ -291,6 +218,7 @@ __global__ void __launch_bounds__(kRowThreads)
       if (lane < 9) {
         // Even steps read slot i of the row upstream of c_i (internal axis 1: the reference's
         // x); odd steps read the row itself.
+        constexpr unsigned kPlus = row_shift_mask(1), kMinus = row_shift_mask(-1);
         const unsigned row = !EVEN ? rowx
                                    : (((kPlus >> lane) & 1u) ? rowm
                                                              : (((kMinus >> lane) & 1u) ? rowp : rowx));
@@ -325,14 +253,6 @@ __global__ void __launch_bounds__(kRowThreads)
       if (bytes) bulk_copy(st + dst, reinterpret_cast<const void*>(lo), bytes, full + s);
       produced = j + 1;
     }
-    // The last rows' results (bounded waits for the consumers), then every store complete.
-    if (ok) {
-      for (int j = produced - S > 0 ? produced - S : 0; j < produced && ok; ++j) {
-        ok = __all_sync(0xffffffffu, mbar_wait(empty + j % S, (unsigned)((j / S) & 1), a.spin_limit));
-        if (ok) store_stage(j % S);
-      }
-    }
-    bulk_wait_all();
     if (!ok && lane == 0) atomicOr(a.status, 2);
     // Leave only once the copies of the last stages have landed (bounded), so that no copy
     // writes into shared memory after the CTA is gone.
@@ -358,12 +278,10 @@ __global__ void __launch_bounds__(kRowThreads)
     const int ny = h.ny;
     const unsigned row0 = h.row[0], row1 = h.row[1], row2 = h.row[2];
     const Real om_p = (Real)h.om_pos, om_n = (Real)h.om_neg;
-    RowStageSink<K> sink;
-    T* const* seg = sink.seg;
+    const T* seg[D2Q9::Q];
 #pragma unroll
     for (int i = 0; i < D2Q9::Q; ++i)
-      sink.seg[i] = reinterpret_cast<T*>(const_cast<unsigned char*>(st) + (size_t)i * St::seg_bytes) +
-                    h.off[i];
+      seg[i] = reinterpret_cast<const T*>(st + (size_t)i * St::seg_bytes) + h.off[i];
     const unsigned char* fl = st + St::off_flags + h.off[9];
     for (int z = tid; z < ny; z += 32 * CW) {
       CellPos c;
@@ -389,9 +307,8 @@ __global__ void __launch_bounds__(kRowThreads)
           fv[i] = P::load(seg[slot] + zi, weight<D2Q9, Real>(i));
       }
       Real g[1];
-      update_cell<D2Q9, TRT, K, EVEN, 0>(a, c, flag, fv, g, Real(0), om_p, om_n, sink);
+      update_cell<D2Q9, TRT, K, EVEN, 0>(a, c, flag, fv, g, Real(0), om_p, om_n);
     }
-    fence_proxy_async();  // this thread's stage writes, visible to the producer's bulk stores
     __syncwarp();
     if (lane == 0) mbar_arrive(empty + s);  // this warp is done with stage s
   }
