@@ -578,11 +578,24 @@ class Reference:
         self.fluid = (flags_t & 7) == 0
 
 
-def coarse_trajectory(cfg: Config, ref: Reference, net: Net | None) -> Trajectory:
+def coarse_trajectory(cfg: Config, ref: Reference, net: Net | None,
+                      uniform_dtau: float | None = None) -> Trajectory:
+    """The coarse run from ref's filtered start: plain (net None), with the closure, or with a
+    spatially uniform relaxation-time correction ``uniform_dtau`` on every fluid cell (the
+    ablation of the network's spatial field: tau = tau0 + uniform_dtau, constant in time)."""
     torch = _torch()
     sim, setup = start_coarse(cfg, ref.rho0.cpu().numpy(), ref.vel0.cpu().numpy(),
                               ref.c0.cpu().numpy())
     run = ClosedRun(sim, setup.flags, net, cfg.every, setup.tau)
+    uniform = None
+    if uniform_dtau is not None:
+        if net is not None:
+            raise ValueError("a uniform correction replaces the network")
+        fluid = torch.tensor((np.asarray(setup.flags) & 7) == 0, device="cuda").reshape(-1)
+        uniform = torch.full((fluid.numel(),), 1.0 / setup.tau, device="cuda")
+        uniform[fluid] = 1.0 / (setup.tau + uniform_dtau)
+        torch.cuda.synchronize()
+        sim._set_omega_field(uniform.data_ptr())
     ext = torch.cuda.ExternalStream(run.stream)
     errors, seconds, done = [], 0.0, 0
     for h in cfg.horizons:
@@ -600,7 +613,52 @@ def coarse_trajectory(cfg: Config, ref: Reference, net: Net | None) -> Trajector
             errors += [float("inf")] * (len(cfg.horizons) - len(errors))
             break
     run.close()
+    if uniform is not None:
+        sim._set_omega_field(0)
     return Trajectory(errors, seconds)
+
+
+def field_mean(cfg: Config, net: Net, ref: Reference) -> float:
+    """Mean relaxation-time correction tau - tau0 the network installs over the fluid cells,
+    averaged over every application of the closed coarse run from ref's start."""
+    torch = _torch()
+    sim, setup = start_coarse(cfg, ref.rho0.cpu().numpy(), ref.vel0.cpu().numpy(),
+                              ref.c0.cpu().numpy())
+    run = ClosedRun(sim, setup.flags, net, cfg.every, setup.tau)
+    fluid = torch.tensor((np.asarray(setup.flags) & 7) == 0, device="cuda").reshape(-1)
+    ext = torch.cuda.ExternalStream(run.stream)
+    total, count = 0.0, 0
+    for _ in range(cfg.horizons[-1] // cfg.every):
+        with torch.cuda.stream(ext):
+            run.apply()
+            total += float((1.0 / run.omega[fluid] - setup.tau).mean())
+        count += 1
+        sim._iterate_device(cfg.every)
+    sim._synchronize()
+    run.close()
+    return total / count
+
+
+def ablation(cfg: Config, net: Net, calib: Reference, test: Reference,
+             factors=(0.25, 0.5, 1.0, 2.0, 4.0)) -> dict:
+    """What the network's spatial field adds over a spatially uniform correction. Judged on the
+    test seed, like the closure: (a) the uniform correction equal to the mean of the network's
+    own field there; (b) the best uniform correction from factors x that mean, picked on the
+    calibration seed. Mean relative velocity L2 errors against the filtered fine run."""
+    mean_dtau = field_mean(cfg, net, test)
+    calibration = {f: coarse_trajectory(cfg, calib, None, f * mean_dtau).mean for f in factors}
+    best = min(calibration, key=lambda f: calibration[f])
+    a = coarse_trajectory(cfg, test, None, mean_dtau)
+    b = coarse_trajectory(cfg, test, None, best * mean_dtau)
+    closed = coarse_trajectory(cfg, test, net)
+    return {
+        "field_mean_dtau": mean_dtau,
+        "calibration_mean_errors": {str(f): e for f, e in calibration.items()},
+        "calibrated_dtau": best * mean_dtau,
+        "uniform_mean": {"dtau": mean_dtau, "errors": a.errors, "mean": a.mean},
+        "uniform_calibrated": {"dtau": best * mean_dtau, "errors": b.errors, "mean": b.mean},
+        "closure": {"errors": closed.errors, "mean": closed.mean},
+    }
 
 
 def calibrate(cfg: Config, net: Net, ref: Reference) -> dict:
