@@ -639,24 +639,32 @@ def field_mean(cfg: Config, net: Net, ref: Reference) -> float:
     return total / count
 
 
+# Uniform corrections tried for the calibrated constant, besides multiples of the network field's
+# mean: from 6% to 60x the coarse set-up's own tau0 - 1/2 (4.8e-4), i.e. a constant eddy
+# viscosity up to well past what the coarse run needs to stay finite.
+UNIFORM_DTAU = (3e-5, 1e-4, 3e-4, 1e-3, 3e-3, 1e-2, 3e-2)
+
+
 def ablation(cfg: Config, net: Net, calib: Reference, test: Reference,
-             factors=(0.25, 0.5, 1.0, 2.0, 4.0)) -> dict:
+             factors=(0.25, 0.5, 1.0, 2.0, 4.0), absolute=UNIFORM_DTAU) -> dict:
     """What the network's spatial field adds over a spatially uniform correction. Judged on the
     test seed, like the closure: (a) the uniform correction equal to the mean of the network's
-    own field there; (b) the best uniform correction from factors x that mean, picked on the
-    calibration seed. Mean relative velocity L2 errors against the filtered fine run."""
+    own field there; (b) the best uniform correction among factors x that mean and the absolute
+    values, picked on the calibration seed. Mean relative velocity L2 errors against the filtered
+    fine run."""
     mean_dtau = field_mean(cfg, net, test)
-    calibration = {f: coarse_trajectory(cfg, calib, None, f * mean_dtau).mean for f in factors}
-    best = min(calibration, key=lambda f: calibration[f])
+    candidates = sorted({f * mean_dtau for f in factors} | set(absolute))
+    calibration = {d: coarse_trajectory(cfg, calib, None, d).mean for d in candidates}
+    best = min(calibration, key=lambda d: calibration[d])
     a = coarse_trajectory(cfg, test, None, mean_dtau)
-    b = coarse_trajectory(cfg, test, None, best * mean_dtau)
+    b = coarse_trajectory(cfg, test, None, best)
     closed = coarse_trajectory(cfg, test, net)
     return {
         "field_mean_dtau": mean_dtau,
-        "calibration_mean_errors": {str(f): e for f, e in calibration.items()},
-        "calibrated_dtau": best * mean_dtau,
+        "calibration_mean_errors": {f"{d:.3g}": e for d, e in calibration.items()},
+        "calibrated_dtau": best,
         "uniform_mean": {"dtau": mean_dtau, "errors": a.errors, "mean": a.mean},
-        "uniform_calibrated": {"dtau": best * mean_dtau, "errors": b.errors, "mean": b.mean},
+        "uniform_calibrated": {"dtau": best, "errors": b.errors, "mean": b.mean},
         "closure": {"errors": closed.errors, "mean": closed.mean},
     }
 
