@@ -641,8 +641,10 @@ def field_mean(cfg: Config, net: Net, ref: Reference) -> float:
 
 # Uniform corrections tried for the calibrated constant, besides multiples of the network field's
 # mean: from 6% to 60x the coarse set-up's own tau0 - 1/2 (4.8e-4), i.e. a constant eddy
-# viscosity up to well past what the coarse run needs to stay finite.
-UNIFORM_DTAU = (3e-5, 1e-4, 3e-4, 1e-3, 3e-3, 1e-2, 3e-2)
+# viscosity up to well past what the coarse run needs to stay finite, with steps of about 1.2x
+# around the smallest values that keep it finite (more dissipation only adds error there).
+UNIFORM_DTAU = (3e-5, 1e-4, 1.2e-4, 1.4e-4, 1.7e-4, 2e-4, 2.4e-4, 3e-4, 4e-4, 6e-4, 1e-3, 3e-3,
+                1e-2, 3e-2)
 
 
 def ablation(cfg: Config, net: Net, calib: Reference, test: Reference,
