@@ -642,11 +642,13 @@ def run_closure(args) -> None:
     net, rep = cl.train(cfg, data)
     S = data.rho.shape[0]
     del data
-    cal = cl.calibrate(cfg, net, cl.Reference(cfg, cfg.calib_seed))
+    calref = cl.Reference(cfg, cfg.calib_seed)
+    cal = cl.calibrate(cfg, net, calref)
     ref = cl.Reference(cfg, cfg.test_seed)
     with ClockSampler(local) as clocks:
         verdict = cl.judge(cfg, net, ref)
     summary = verdict.summary()
+    ablation = cl.ablation(cfg, net, calref, ref)  # the network field against uniform ones
     t1 = time.perf_counter()
     kind, _ = cl.run_closed_or_fine(cfg, verdict, net, ref)
     e2e_s = time.perf_counter() - t1
@@ -717,6 +719,7 @@ def run_closure(args) -> None:
         },
         "closure": summary,
         "calibration": cal,
+        "ablation_uniform_correction": ablation,
         "fused_relaxation": {
             "us_per_application": fused_s * 1e6,
             "tflops": 21_312.0 * nx * ny / fused_s / 1e12,
