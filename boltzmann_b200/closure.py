@@ -53,12 +53,20 @@ _SIGS = {
     "lbm_closure_relaxation": [_P, _P, _P, _P, _P, _I64, _I64, _P, _F, _F, _F, _P, _P],
     "lbm_closure_status": [],
     "lbm_closure_set_spin_limit": [_I64],
+    "lbm_closure_set_layer2_kernel": [_I],
 }
 for _name, _args in _SIGS.items():
     getattr(_lib, _name).argtypes = _args
     getattr(_lib, _name).restype = C.c_int
 
 NPARAMS = 10721
+LAYER2_KERNELS = {"tcgen05": 0, "warp_mma": 1}
+
+
+def set_layer2_kernel(kind: str) -> None:
+    """Selects the kernel of layer 2 in training (forward and the transposed conv): "tcgen05"
+    (default) or "warp_mma"; process-wide."""
+    _check(_lib.lbm_closure_set_layer2_kernel(LAYER2_KERNELS[kind]))
 CHANNELS = 32
 
 

@@ -6,8 +6,9 @@
 //
 //   layer   forward                       backward
 //   1 (4->32)   CUDA cores (36 MAC/out)    weights: CUDA cores; no input gradient
-//   2 (32->32)  mma.sync BF16, FP32 acc    data: mma.sync (transposed conv, fused GELU');
-//                                          weights: mma.sync (cells are the reduction axis)
+//   2 (32->32)  tcgen05 BF16, FP32 acc     data: tcgen05 (transposed conv, fused GELU');
+//               (TMEM accumulators)        weights: mma.sync (cells are the reduction axis)
+//               mma.sync kept selectable (lbm_closure_set_layer2_kernel)
 //   3 (32->1)   CUDA cores                 data + weights: CUDA cores (fused GELU')
 //
 // Every product sum takes BF16 operands (weights, activations, pre-activation gradients rounded
@@ -1248,6 +1249,245 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
 }
 
 // ---------------------------------------------------------------------------------------------
+// Layer 2 of the training path on tcgen05: the forward conv (BWD = false: z2 = b2 + W * a1,
+// a2 = GELU(z2) in BF16) and the transposed conv of the backward pass (BWD = true:
+// d = W^T * dz2, dz1 = BF16(d GELU'(z1)), plus the per-channel sums of dz1 for the layer-1 bias
+// gradient in this CTA's partial row). Same products as conv32_kernel, on the fifth-generation
+// tensor cores with the layout of the fused inference kernel's layer 2:
+//   - a tile of kTR x kTC output cells reads a (kTR + 2) x (kTC + 2) input region, staged
+//     chunk-major: plane k (channels 8k .. 8k+7) holds 16 bytes a cell, cells in row-major order
+//     of the region, so a tap shift (dx, dy) of the 3x3 stencil is an offset of the descriptor's
+//     start address, dx (kTC + 2) + dy cells (the negated shift for the transposed conv);
+//   - kTBlocks blocks of 128 consecutive region cells starting at output cell (0, 0), each an
+//     M = 128, N = 32, K = 288 product into its own 32 TMEM columns; rows that fall on the
+//     region's first or last column are computed and discarded;
+//   - the B operand is the weights as K-chunks of 8: [k chunk][n][8] with k = (tap, ci) and
+//     n = co for the forward conv, k = (tap, co) and n = ci for the transposed one.
+// One thread issues the MMAs and commits them to an mbarrier (bounded wait, as everywhere); the
+// epilogue reads each cell's 32 accumulators with tcgen05.ld. Two CTAs share an SM, so one stages
+// its next tile while the other's MMAs and epilogue run.
+
+constexpr int kTR = 14, kTC = 64;                  // output tile
+constexpr int kTRegR = kTR + 2, kTRegC = kTC + 2;  // input region
+constexpr int kTFirst = kTRegC + 1;                // region index of output cell (0, 0)
+constexpr int kTBlocks = (kTR * kTRegC + 127) / 128;  // 128-cell blocks covering the output rows
+constexpr int kTPad = 1161;  // cells per plane: >= kTFirst + 128 kTBlocks + kTRegC + 1, and odd so
+                             // that the four planes start in different 16-byte bank groups
+constexpr int kTThreads = 256;
+constexpr int kTTmemCols = 256;  // 8 accumulators of 32 FP32 columns
+constexpr size_t kTOffW = (size_t)4 * kTPad * 16;
+constexpr size_t kTOffBias = kTOffW + (size_t)36 * C * 16;
+constexpr size_t kTOffBar = kTOffBias + (size_t)C * 4;
+constexpr size_t kTSmem = kTOffBar + 16;
+static_assert((size_t)kTThreads * (C + 1) * 4 <= kTOffW, "bias partial sums must fit the region");
+static_assert(kTBlocks * 32 <= kTTmemCols, "accumulators exceed the TMEM allocation");
+static_assert(kTFirst + kTBlocks * 128 + kTRegC + 1 <= kTPad, "planes too short for the shifts");
+static_assert(kTFirst + kTBlocks * 128 - 1 >= (kTR * kTRegC) + kTC, "blocks do not cover the tile");
+static_assert(kTFirst - kTRegC - 1 >= 0, "a negative shift leaves the plane");
+
+template <bool BWD>
+__global__ void __launch_bounds__(kTThreads, 2)
+    conv32_tc_kernel(Grid g, const bf16* __restrict__ in, const bf16* __restrict__ w2,
+                     const float* __restrict__ bias, const float* __restrict__ zin,
+                     float* __restrict__ zout, bf16* __restrict__ out, float* __restrict__ partial) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* ac = smem_raw;                    // [4 planes][kTPad cells][16 B]
+  unsigned char* wc = smem_raw + kTOffW;           // [36 K-chunks][32 n][16 B]
+  float* bs = reinterpret_cast<float*>(smem_raw + kTOffBias);  // forward: b2
+  uint64_t* mma_done = reinterpret_cast<uint64_t*>(smem_raw + kTOffBar);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem_raw + kTOffBar + 8);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int kWarps = kTThreads / 32;
+
+  // The B operand. Forward: chunk kk = (tap, ci chunk) of output channel co, 8 consecutive
+  // weights of the [co][288] row. Transposed: chunk kk = (tap, co chunk) of input channel ci,
+  // weights W[8 cc .. 8 cc + 7][tap][ci].
+  for (int i = threadIdx.x; i < 36 * C; i += blockDim.x) {
+    const int kk = i / C, n = i - kk * C;
+    if (!BWD) {
+      *reinterpret_cast<uint4*>(wc + (size_t)i * 16) =
+          __ldg(reinterpret_cast<const uint4*>(w2 + n * 288 + kk * 8));
+    } else {
+      const int tap = kk >> 2, cc = kk & 3;
+      bf16 v[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) v[j] = w2[(cc * 8 + j) * 288 + tap * 32 + n];
+      *reinterpret_cast<uint4*>(wc + (size_t)i * 16) = *reinterpret_cast<const uint4*>(v);
+    }
+  }
+  if (!BWD && threadIdx.x < C) bs[threadIdx.x] = bias[threadIdx.x];
+  // Plane cells past the region feed only discarded rows; keep them finite.
+  for (int i = threadIdx.x; i < 4 * kTPad; i += blockDim.x)
+    if (i % kTPad >= kTRegR * kTRegC)
+      *reinterpret_cast<uint4*>(ac + (size_t)i * 16) = make_uint4(0, 0, 0, 0);
+  if (threadIdx.x == 0) {
+    cl_mbar_init(mma_done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(tmem_slot)),
+                 "r"(kTTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t idesc = umma_idesc_bf16(128, 32);
+  const unsigned ac_addr = smem_addr(ac), wc_addr = smem_addr(wc);
+  const unsigned spin_limit = g_closure_spin_limit;
+  bool healthy = true;
+  unsigned phase = 0;
+  float bias_sum[C];  // BWD: this thread's running sums of dz1 per channel
+#pragma unroll
+  for (int c = 0; c < C; ++c) bias_sum[c] = 0.0f;
+
+  for (int64_t t = blockIdx.x; t < g.tiles && healthy; t += gridDim.x) {
+    int64_t b, x0, y0;
+    {
+      const int64_t per = g.tx * g.ty;  // this kernel's tiles are kTR x kTC (see the launcher)
+      b = t / per;
+      const int64_t r = t - b * per;
+      x0 = (r / g.ty) * kTR;
+      y0 = (r % g.ty) * kTC;
+    }
+    // Stage the input region (zero outside the domain), chunk-major.
+    for (int i = threadIdx.x; i < kTRegR * kTRegC * 4; i += blockDim.x) {
+      const int chunk = i & 3, cell = i >> 2;
+      const int r = cell / kTRegC, c = cell - r * kTRegC;
+      const int64_t x = x0 - 1 + r, y = y0 - 1 + c;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (x >= 0 && x < g.nx && y >= 0 && y < g.ny)
+        v = __ldg(reinterpret_cast<const uint4*>(in + g.cell(b, x, y) * C) + chunk);
+      *reinterpret_cast<uint4*>(ac + ((size_t)chunk * kTPad + cell) * 16) = v;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the MMAs
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tc_fence_after();
+      // K-slice outer, block inner: consecutive MMAs accumulate into different TMEM columns.
+#pragma unroll 1
+      for (int tap = 0; tap < 9; ++tap) {
+        const int sh = (tap / 3 - 1) * kTRegC + (tap % 3 - 1);
+        const int off = BWD ? -sh : sh;
+#pragma unroll
+        for (int kc = 0; kc < 2; ++kc) {
+          const int sidx = tap * 2 + kc;
+          const uint64_t bdesc = umma_desc(wc_addr + (unsigned)(sidx * 1024), C * 16, 128);
+          const unsigned a_base = ac_addr + (unsigned)((2 * kc * kTPad + kTFirst + off) * 16);
+#pragma unroll
+          for (int m = 0; m < kTBlocks; ++m)
+            umma_bf16(tmem + (uint32_t)(m * 32),
+                      umma_desc(a_base + (unsigned)(m * 128 * 16), kTPad * 16, 128), bdesc, idesc,
+                      sidx != 0);
+        }
+      }
+      umma_commit(mma_done);
+    }
+    const bool got = cl_mbar_wait(mma_done, phase, spin_limit);
+    phase ^= 1u;
+    if (!__syncthreads_and(got)) {
+      healthy = false;
+      break;
+    }
+    tc_fence_after();
+    // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its sub-partition) of blocks
+    // w / 4, w / 4 + 2, ...; one thread per cell, its 32 channels in registers.
+    for (int m = warp >> 2; m < kTBlocks; m += kWarps / 4) {
+      const int sp = warp & 3;
+      uint32_t r32[32];
+      tmem_ld32(tmem + ((uint32_t)(32 * sp) << 16) + (uint32_t)(m * 32), r32);
+      const int q = kTFirst + 128 * m + 32 * sp + lane;  // region index of this row
+      const int r = q / kTRegC - 1, c = q % kTRegC - 1;   // output tile coordinates
+      if (r < 0 || r >= kTR || c < 0 || c >= kTC) continue;
+      const int64_t x = x0 + r, y = y0 + c;
+      if (x >= g.nx || y >= g.ny) continue;
+      const int64_t cell = g.cell(b, x, y);
+      uint32_t packed[C / 2];
+      if (!BWD) {
+        float z[C];
+#pragma unroll
+        for (int ch = 0; ch < C; ++ch) z[ch] = __uint_as_float(r32[ch]) + bs[ch];
+        if (zout != nullptr) {
+          float4* zp = reinterpret_cast<float4*>(zout + cell * C);
+#pragma unroll
+          for (int k = 0; k < C / 4; ++k)
+            zp[k] = make_float4(z[4 * k], z[4 * k + 1], z[4 * k + 2], z[4 * k + 3]);
+        }
+#pragma unroll
+        for (int ch = 0; ch < C; ch += 2)
+          packed[ch / 2] = (uint32_t)__bfloat16_as_ushort(to_bf(gelu(z[ch]))) |
+                           ((uint32_t)__bfloat16_as_ushort(to_bf(gelu(z[ch + 1]))) << 16);
+      } else {
+        const float4* zp = reinterpret_cast<const float4*>(zin + cell * C);
+#pragma unroll
+        for (int k = 0; k < C / 4; ++k) {
+          const float4 zz = zp[k];
+          const float zv[4] = {zz.x, zz.y, zz.z, zz.w};
+#pragma unroll
+          for (int e = 0; e < 4; e += 2) {
+            const int ch = 4 * k + e;
+            const bf16 o0 = to_bf(__uint_as_float(r32[ch]) * gelu_grad(zv[e]));
+            const bf16 o1 = to_bf(__uint_as_float(r32[ch + 1]) * gelu_grad(zv[e + 1]));
+            bias_sum[ch] += bf(o0);
+            bias_sum[ch + 1] += bf(o1);
+            packed[ch / 2] =
+                (uint32_t)__bfloat16_as_ushort(o0) | ((uint32_t)__bfloat16_as_ushort(o1) << 16);
+          }
+        }
+      }
+      uint4* op = reinterpret_cast<uint4*>(out + cell * C);
+#pragma unroll
+      for (int k = 0; k < C / 8; ++k)
+        op[k] = make_uint4(packed[4 * k], packed[4 * k + 1], packed[4 * k + 2], packed[4 * k + 3]);
+    }
+    tc_fence_before();
+    __syncthreads();  // the region and every TMEM column are free for the next tile
+  }
+  if (!healthy) {
+    if (threadIdx.x == 0) {
+      atomicOr(&g_closure_status, 1);
+      cl_mbar_wait(mma_done, phase ^ 1u);  // give MMAs still in flight a bounded chance to end
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTTmemCols)
+                 : "memory");
+  }
+  if (BWD) {
+    // Per-channel sums of this CTA's dz1 in a fixed order: thread sums in the region area (free
+    // now; rows padded to C + 1 against bank conflicts), then channel c adds the 256 threads'
+    // values in thread order.
+    float* sums = reinterpret_cast<float*>(ac);  // [kTThreads][C + 1]
+#pragma unroll
+    for (int c = 0; c < C; ++c) sums[threadIdx.x * (C + 1) + c] = bias_sum[c];
+    __syncthreads();
+    if (threadIdx.x < C) {
+      float s = 0.0f;
+      for (int k = 0; k < kTThreads; ++k) s += sums[k * (C + 1) + threadIdx.x];
+      partial[(int64_t)blockIdx.x * LBM_CLOSURE_PARAMS + LBM_CLOSURE_OFF_B1 + threadIdx.x] = s;
+    }
+  }
+}
+
+// Tiles of kTR x kTC cells for conv32_tc_kernel.
+Grid tc_grid(int64_t nx, int64_t ny, int64_t batch) {
+  Grid g{nx, ny, batch, (nx + kTR - 1) / kTR, (ny + kTC - 1) / kTC, 0};
+  g.tiles = g.tx * g.ty * batch;
+  return g;
+}
+
+// Which kernel runs layer 2 of the training path (lbm_closure_set_layer2_kernel).
+int g_layer2_kernel = LBM_CLOSURE_LAYER2_TCGEN05;
+
+// ---------------------------------------------------------------------------------------------
 // Optimiser, relaxation field, coarsening
 
 __global__ void adam_kernel(float* __restrict__ p, bf16* __restrict__ pb, const float* __restrict__ g,
@@ -1402,6 +1642,7 @@ int lbm_closure_forward(const float* params, const uint16_t* params_bf16, const 
   if (!configured) {
     if (int rc = set_smem((const void*)conv32_kernel<false>, kConv32Smem)) return rc;
     if (int rc = set_smem((const void*)conv32_kernel<true>, kConv32Smem)) return rc;
+    if (int rc = set_smem((const void*)conv32_tc_kernel<false>, kTSmem)) return rc;
     if (int rc = set_smem((const void*)conv3_fwd_kernel, kConv3Smem)) return rc;
     configured = true;
   }
@@ -1414,10 +1655,18 @@ int lbm_closure_forward(const float* params, const uint16_t* params_bf16, const 
                                               wb + LBM_CLOSURE_OFF_W1, params + LBM_CLOSURE_OFF_B1,
                                               z1, reinterpret_cast<bf16*>(a1));
   CL_CUDA(cudaGetLastError());
-  const int grid32 = (int)std::min<int64_t>(g.tiles, (int64_t)sms * 4);
-  conv32_kernel<false><<<grid32, kConv32Threads, kConv32Smem, s>>>(
-      g, reinterpret_cast<const bf16*>(a1), wb + LBM_CLOSURE_OFF_W2, params + LBM_CLOSURE_OFF_B2,
-      nullptr, z2, reinterpret_cast<bf16*>(a2), nullptr);
+  if (g_layer2_kernel == LBM_CLOSURE_LAYER2_TCGEN05) {
+    const Grid gt = tc_grid(nx, ny, batch);
+    const int grid_tc = (int)std::min<int64_t>(gt.tiles, (int64_t)sms * 2);
+    conv32_tc_kernel<false><<<grid_tc, kTThreads, kTSmem, s>>>(
+        gt, reinterpret_cast<const bf16*>(a1), wb + LBM_CLOSURE_OFF_W2,
+        params + LBM_CLOSURE_OFF_B2, nullptr, z2, reinterpret_cast<bf16*>(a2), nullptr);
+  } else {
+    const int grid32 = (int)std::min<int64_t>(g.tiles, (int64_t)sms * 4);
+    conv32_kernel<false><<<grid32, kConv32Threads, kConv32Smem, s>>>(
+        g, reinterpret_cast<const bf16*>(a1), wb + LBM_CLOSURE_OFF_W2,
+        params + LBM_CLOSURE_OFF_B2, nullptr, z2, reinterpret_cast<bf16*>(a2), nullptr);
+  }
   CL_CUDA(cudaGetLastError());
   conv3_fwd_kernel<<<grid_small, 256, kConv3Smem, s>>>(g, reinterpret_cast<const bf16*>(a2),
                                                        wb + LBM_CLOSURE_OFF_W3,
@@ -1465,6 +1714,7 @@ int lbm_closure_backward(const float* params, const uint16_t* params_bf16, const
   if (!configured) {
     if (int rc = set_smem((const void*)conv32_kernel<false>, kConv32Smem)) return rc;
     if (int rc = set_smem((const void*)conv32_kernel<true>, kConv32Smem)) return rc;
+    if (int rc = set_smem((const void*)conv32_tc_kernel<true>, kTSmem)) return rc;
     if (int rc = set_smem((const void*)conv32_wgrad_kernel, kDw2Smem)) return rc;
     if (int rc = set_smem((const void*)conv3_bwd_kernel, kConv3BwdSmem)) return rc;
     configured = true;
@@ -1485,8 +1735,15 @@ int lbm_closure_backward(const float* params, const uint16_t* params_bf16, const
   conv32_wgrad_kernel<<<rows, kDw2Threads, kDw2Smem, s>>>(g, reinterpret_cast<const bf16*>(a1),
                                                           dz2, partial);
   CL_CUDA(cudaGetLastError());
-  conv32_kernel<true><<<rows, kConv32Threads, kConv32Smem, s>>>(
-      g, dz2, wb + LBM_CLOSURE_OFF_W2, nullptr, z1, nullptr, dz1, partial);
+  if (g_layer2_kernel == LBM_CLOSURE_LAYER2_TCGEN05) {
+    // Same number of CTAs (partial rows) as the other reducing kernels: a CTA without a tile
+    // writes a zero row.
+    conv32_tc_kernel<true><<<rows, kTThreads, kTSmem, s>>>(
+        tc_grid(nx, ny, batch), dz2, wb + LBM_CLOSURE_OFF_W2, nullptr, z1, nullptr, dz1, partial);
+  } else {
+    conv32_kernel<true><<<rows, kConv32Threads, kConv32Smem, s>>>(
+        g, dz2, wb + LBM_CLOSURE_OFF_W2, nullptr, z1, nullptr, dz1, partial);
+  }
   CL_CUDA(cudaGetLastError());
   conv1_wgrad_kernel<<<rows, 288, kTX * kTY * kCS * sizeof(bf16), s>>>(
       g, reinterpret_cast<const bf16*>(x), dz1, partial);
@@ -1562,6 +1819,13 @@ int lbm_closure_relaxation(const float* params, const uint16_t* params_bf16, con
   const int grid = (int)std::min<int64_t>(ntiles, (int64_t)device_sms());
   closure_fused_kernel<<<grid, kFusedThreads, kFusedSmem, (cudaStream_t)stream>>>(fa);
   CL_CUDA(cudaGetLastError());
+  return LBM_OK;
+}
+
+int lbm_closure_set_layer2_kernel(int kind) {
+  if (kind != LBM_CLOSURE_LAYER2_TCGEN05 && kind != LBM_CLOSURE_LAYER2_WARP_MMA)
+    return fail(LBM_ERR_ARGUMENT, "unknown layer-2 kernel");
+  g_layer2_kernel = kind;
   return LBM_OK;
 }
 

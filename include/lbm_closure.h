@@ -123,6 +123,15 @@ LBM_API int lbm_closure_relaxation(const float* params, const uint16_t* params_b
                                    int64_t nx, int64_t ny, const float* norm, float tau0,
                                    float gain, float max_dtau, float* omega, void* stream);
 
+/* Which kernel runs layer 2 (32 -> 32 channels) of lbm_closure_forward and the transposed conv of
+ * lbm_closure_backward, process-wide: LBM_CLOSURE_LAYER2_TCGEN05 (default; fifth-generation tensor
+ * cores, accumulators in tensor memory) or LBM_CLOSURE_LAYER2_WARP_MMA (warp-level mma.sync). Both
+ * take BF16 operands and accumulate in FP32; they differ only in summation order. No reference
+ * counterpart. */
+#define LBM_CLOSURE_LAYER2_TCGEN05 0
+#define LBM_CLOSURE_LAYER2_WARP_MMA 1
+LBM_API int lbm_closure_set_layer2_kernel(int kind);
+
 /* Polls that the lbm_closure_relaxation kernel makes, on the current device, while waiting for
  * its tensor-core products before it gives up (polls < 0: the default, 2^22). A kernel that gives
  * up records it for lbm_closure_status, still waits (with the default bound) for the products in

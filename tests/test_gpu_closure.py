@@ -101,8 +101,16 @@ def _rel(a, b):
     return float(np.linalg.norm(np.ravel(a - b)) / max(np.linalg.norm(np.ravel(b)), 1e-30))
 
 
+@pytest.fixture(params=["tcgen05", "warp_mma"])
+def layer2(request, cl):
+    """Runs a test with each kernel of layer 2 (training forward and transposed conv)."""
+    cl.set_layer2_kernel(request.param)
+    yield request.param
+    cl.set_layer2_kernel("tcgen05")
+
+
 @pytest.mark.parametrize("B,nx,ny", SHAPES)
-def test_forward_layers_match_oracle(torch, cl, B, nx, ny):
+def test_forward_layers_match_oracle(torch, cl, B, nx, ny, layer2):
     """Each layer from the GPU's own (BF16) input: FP32 accumulation of BF16 products against a
     float64 sum of the same products; BF16 outputs may differ by one unit where the FP32 value
     sits on a rounding boundary."""
@@ -125,8 +133,8 @@ def test_forward_layers_match_oracle(torch, cl, B, nx, ny):
     assert _rel(g["y"], ref["y"]) < 5e-3
 
 
-@pytest.mark.parametrize("B,nx,ny", SHAPES)
-def test_loss_and_gradient_match_oracle(torch, cl, B, nx, ny):
+@pytest.mark.parametrize("B,nx,ny", SHAPES + [(2, 30, 130)])
+def test_loss_and_gradient_match_oracle(torch, cl, B, nx, ny, layer2):
     net, bufs, flags, flags_t, params, x, g = _forward(torch, cl, B, nx, ny, seed=3)
     rng = np.random.default_rng(9)
     target = rng.normal(size=(B, nx, ny)).astype(np.float32)
@@ -282,3 +290,26 @@ def test_fused_relaxation_matches_layered_kernels(torch, cl, nx, ny):
     assert (a[fixed_or_wall] == np.float32(1.0) / np.float32(0.51)).all()
     # the network's output really varies the rate inside the fluid
     assert np.ptp(a[~fixed_or_wall]) > 1e-3
+
+
+def test_layer2_kernels_agree(torch, cl):
+    """The tcgen05 and the warp-MMA kernels of layer 2 compute the same products in a different
+    summation order: z2 within FP32 accumulation noise, the BF16 activations and every gradient
+    block nearly identical."""
+    B, nx, ny = 2, 40, 150  # several 14 x 64 and 4 x 64 tiles, partial ones at both edges
+    runs = {}
+    for kind in ("warp_mma", "tcgen05"):
+        cl.set_layer2_kernel(kind)
+        net, bufs, flags, flags_t, params, x, g = _forward(torch, cl, B, nx, ny, seed=5)
+        rng = np.random.default_rng(4)
+        tt = torch.tensor(rng.normal(size=(B, nx, ny)).astype(np.float32), device="cuda")
+        cl.loss_and_grad(net, bufs, tt.reshape(-1), flags_t, 0)
+        torch.cuda.synchronize()
+        runs[kind] = (g, bufs.grad.cpu().numpy().astype(np.float64))
+    cl.set_layer2_kernel("tcgen05")
+    (ga, grad_a), (gb, grad_b) = runs["warp_mma"], runs["tcgen05"]
+    assert np.abs(ga["z2"] - gb["z2"]).max() <= 1e-5 * max(1.0, np.abs(ga["z2"]).max())
+    assert np.mean(ga["a2"] != gb["a2"]) < 1e-3
+    assert _rel(gb["y"], ga["y"]) < 1e-3
+    for lo, hi in ((0, 1152), (1152, 1184), (1184, 10400), (10400, 10432), (10432, 10721)):
+        assert _rel(grad_b[lo:hi], grad_a[lo:hi]) < 5e-3, (lo, hi)
