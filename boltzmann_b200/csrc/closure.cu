@@ -19,8 +19,10 @@
 // BF16 per cell (80 bytes): eight consecutive cells then start in eight different 16-byte bank
 // groups, so ldmatrix reads them without conflicts. Weight rows (one per output channel) are
 // padded from 288 to 296 BF16 (592 bytes) for the same reason.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -1271,31 +1273,54 @@ constexpr int kTR = 14, kTC = 64;                  // output tile
 constexpr int kTRegR = kTR + 2, kTRegC = kTC + 2;  // input region
 constexpr int kTFirst = kTRegC + 1;                // region index of output cell (0, 0)
 constexpr int kTBlocks = (kTR * kTRegC + 127) / 128;  // 128-cell blocks covering the output rows
-constexpr int kTPad = 1161;  // cells per plane: >= kTFirst + 128 kTBlocks + kTRegC + 1, and odd so
-                             // that the four planes start in different 16-byte bank groups
+constexpr int kTPad = 1168;  // cells per plane: >= kTFirst + 128 kTBlocks + kTRegC + 1, and a
+                             // multiple of 8 so that every plane starts on a 128-byte boundary
 constexpr int kTThreads = 256;
 constexpr int kTTmemCols = 256;  // 8 accumulators of 32 FP32 columns
 constexpr size_t kTOffW = (size_t)4 * kTPad * 16;
 constexpr size_t kTOffBias = kTOffW + (size_t)36 * C * 16;
-constexpr size_t kTOffBar = kTOffBias + (size_t)C * 4;
-constexpr size_t kTSmem = kTOffBar + 16;
+constexpr size_t kTOffBar = kTOffBias + (size_t)C * 4;  // MMA mbarrier, load mbarrier, TMEM addr
+constexpr size_t kTSmem = kTOffBar + 24;
+constexpr unsigned kTLoadBytes = 4u * kTRegR * kTRegC * 16;  // the four plane boxes of a tile
 static_assert((size_t)kTThreads * (C + 1) * 4 <= kTOffW, "bias partial sums must fit the region");
 static_assert(kTBlocks * 32 <= kTTmemCols, "accumulators exceed the TMEM allocation");
 static_assert(kTFirst + kTBlocks * 128 + kTRegC + 1 <= kTPad, "planes too short for the shifts");
 static_assert(kTFirst + kTBlocks * 128 - 1 >= (kTR * kTRegC) + kTC, "blocks do not cover the tile");
 static_assert(kTFirst - kTRegC - 1 >= 0, "a negative shift leaves the plane");
 
+// One plane of a tile's input region by the tensor engine: the activations as a 5D tensor
+// (8 channels, 4 channel chunks, y, x, batch), box {8, 1, kTRegC, kTRegR, 1} at (0, chunk,
+// y0 - 1, x0 - 1, b), which lands as kTRegR x kTRegC cells of 16 bytes in row-major order;
+// cells outside the domain read as zero (the box may start at -1).
+__device__ __forceinline__ void tc_plane_copy(void* dst, const CUtensorMap* map, int chunk, int y,
+                                              int x, int b, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], "
+      "[%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(chunk), "r"(y), "r"(x), "r"(b),
+      "r"(smem_addr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
 template <bool BWD>
 __global__ void __launch_bounds__(kTThreads, 2)
-    conv32_tc_kernel(Grid g, const bf16* __restrict__ in, const bf16* __restrict__ w2,
-                     const float* __restrict__ bias, const float* __restrict__ zin,
-                     float* __restrict__ zout, bf16* __restrict__ out, float* __restrict__ partial) {
+    conv32_tc_kernel(Grid g, const __grid_constant__ CUtensorMap in_map,
+                     const bf16* __restrict__ w2, const float* __restrict__ bias,
+                     const float* __restrict__ zin, float* __restrict__ zout,
+                     bf16* __restrict__ out, float* __restrict__ partial) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* ac = smem_raw;                    // [4 planes][kTPad cells][16 B]
   unsigned char* wc = smem_raw + kTOffW;           // [36 K-chunks][32 n][16 B]
   float* bs = reinterpret_cast<float*>(smem_raw + kTOffBias);  // forward: b2
   uint64_t* mma_done = reinterpret_cast<uint64_t*>(smem_raw + kTOffBar);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem_raw + kTOffBar + 8);
+  uint64_t* loaded = reinterpret_cast<uint64_t*>(smem_raw + kTOffBar + 8);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem_raw + kTOffBar + 16);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int kWarps = kTThreads / 32;
 
@@ -1320,8 +1345,11 @@ __global__ void __launch_bounds__(kTThreads, 2)
   for (int i = threadIdx.x; i < 4 * kTPad; i += blockDim.x)
     if (i % kTPad >= kTRegR * kTRegC)
       *reinterpret_cast<uint4*>(ac + (size_t)i * 16) = make_uint4(0, 0, 0, 0);
+  // The weights and the zeroed plane tails, written here, are read by the MMAs (async proxy).
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   if (threadIdx.x == 0) {
     cl_mbar_init(mma_done, 1);
+    cl_mbar_init(loaded, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -1339,7 +1367,7 @@ __global__ void __launch_bounds__(kTThreads, 2)
   const unsigned ac_addr = smem_addr(ac), wc_addr = smem_addr(wc);
   const unsigned spin_limit = g_closure_spin_limit;
   bool healthy = true;
-  unsigned phase = 0;
+  unsigned phase = 0, load_phase = 0;
   float bias_sum[C];  // BWD: this thread's running sums of dz1 per channel
 #pragma unroll
   for (int c = 0; c < C; ++c) bias_sum[c] = 0.0f;
@@ -1353,19 +1381,20 @@ __global__ void __launch_bounds__(kTThreads, 2)
       x0 = (r / g.ty) * kTR;
       y0 = (r % g.ty) * kTC;
     }
-    // Stage the input region (zero outside the domain), chunk-major.
-    for (int i = threadIdx.x; i < kTRegR * kTRegC * 4; i += blockDim.x) {
-      const int chunk = i & 3, cell = i >> 2;
-      const int r = cell / kTRegC, c = cell - r * kTRegC;
-      const int64_t x = x0 - 1 + r, y = y0 - 1 + c;
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if (x >= 0 && x < g.nx && y >= 0 && y < g.ny)
-        v = __ldg(reinterpret_cast<const uint4*>(in + g.cell(b, x, y) * C) + chunk);
-      *reinterpret_cast<uint4*>(ac + ((size_t)chunk * kTPad + cell) * 16) = v;
+    // The input region, chunk-major, by four tensor copies (zero outside the domain).
+    if (threadIdx.x == 0) {
+      tc_expect_tx(loaded, kTLoadBytes);
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        tc_plane_copy(ac + (size_t)k * kTPad * 16, &in_map, k, (int)y0 - 1, (int)x0 - 1, (int)b,
+                      loaded);
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the MMAs
-    tc_fence_before();
-    __syncthreads();
+    const bool have = cl_mbar_wait(loaded, load_phase);  // the copies take no spin limit: the
+    load_phase ^= 1u;                                     // tile's MMAs need them
+    if (!__syncthreads_and(have)) {
+      healthy = false;
+      break;
+    }
     if (threadIdx.x == 0) {
       tc_fence_after();
       // K-slice outer, block inner: consecutive MMAs accumulate into different TMEM columns.
@@ -1450,7 +1479,9 @@ __global__ void __launch_bounds__(kTThreads, 2)
   if (!healthy) {
     if (threadIdx.x == 0) {
       atomicOr(&g_closure_status, 1);
-      cl_mbar_wait(mma_done, phase ^ 1u);  // give MMAs still in flight a bounded chance to end
+      // Give the copies and MMAs still in flight a bounded chance to end.
+      cl_mbar_wait(loaded, load_phase ^ 1u);
+      cl_mbar_wait(mma_done, phase ^ 1u);
     }
   }
   tc_fence_before();
@@ -1475,6 +1506,29 @@ __global__ void __launch_bounds__(kTThreads, 2)
       partial[(int64_t)blockIdx.x * LBM_CLOSURE_PARAMS + LBM_CLOSURE_OFF_B1 + threadIdx.x] = s;
     }
   }
+}
+
+// The [batch][nx][ny][32] BF16 activations as conv32_tc_kernel's 5D tensor map (through the
+// runtime's driver entry point: no link against libcuda). False when it cannot be encoded.
+bool tc_input_map(CUtensorMap* map, const void* base, int64_t nx, int64_t ny, int64_t batch) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  if (encode == nullptr || (reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
+  if (nx >= (1ll << 31) || ny >= (1ll << 31) || batch >= (1ll << 31)) return false;
+  const cuuint64_t dims[5] = {8, 4, (cuuint64_t)ny, (cuuint64_t)nx, (cuuint64_t)batch};
+  const cuuint64_t strides[4] = {16, 64, (cuuint64_t)ny * 64, (cuuint64_t)(nx * ny) * 64};
+  const cuuint32_t box[5] = {8, 1, (cuuint32_t)kTRegC, (cuuint32_t)kTRegR, 1};
+  const cuuint32_t elem[5] = {1, 1, 1, 1, 1};
+  return encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(base), dims, strides,
+                box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // Tiles of kTR x kTC cells for conv32_tc_kernel.
@@ -1655,12 +1709,13 @@ int lbm_closure_forward(const float* params, const uint16_t* params_bf16, const 
                                               wb + LBM_CLOSURE_OFF_W1, params + LBM_CLOSURE_OFF_B1,
                                               z1, reinterpret_cast<bf16*>(a1));
   CL_CUDA(cudaGetLastError());
-  if (g_layer2_kernel == LBM_CLOSURE_LAYER2_TCGEN05) {
+  CUtensorMap a1_map;
+  if (g_layer2_kernel == LBM_CLOSURE_LAYER2_TCGEN05 && tc_input_map(&a1_map, a1, nx, ny, batch)) {
     const Grid gt = tc_grid(nx, ny, batch);
     const int grid_tc = (int)std::min<int64_t>(gt.tiles, (int64_t)sms * 2);
     conv32_tc_kernel<false><<<grid_tc, kTThreads, kTSmem, s>>>(
-        gt, reinterpret_cast<const bf16*>(a1), wb + LBM_CLOSURE_OFF_W2,
-        params + LBM_CLOSURE_OFF_B2, nullptr, z2, reinterpret_cast<bf16*>(a2), nullptr);
+        gt, a1_map, wb + LBM_CLOSURE_OFF_W2, params + LBM_CLOSURE_OFF_B2, nullptr, z2,
+        reinterpret_cast<bf16*>(a2), nullptr);
   } else {
     const int grid32 = (int)std::min<int64_t>(g.tiles, (int64_t)sms * 4);
     conv32_kernel<false><<<grid32, kConv32Threads, kConv32Smem, s>>>(
@@ -1735,11 +1790,13 @@ int lbm_closure_backward(const float* params, const uint16_t* params_bf16, const
   conv32_wgrad_kernel<<<rows, kDw2Threads, kDw2Smem, s>>>(g, reinterpret_cast<const bf16*>(a1),
                                                           dz2, partial);
   CL_CUDA(cudaGetLastError());
-  if (g_layer2_kernel == LBM_CLOSURE_LAYER2_TCGEN05) {
+  CUtensorMap dz2_map;
+  if (g_layer2_kernel == LBM_CLOSURE_LAYER2_TCGEN05 && tc_input_map(&dz2_map, dz2, nx, ny, batch)) {
     // Same number of CTAs (partial rows) as the other reducing kernels: a CTA without a tile
     // writes a zero row.
     conv32_tc_kernel<true><<<rows, kTThreads, kTSmem, s>>>(
-        tc_grid(nx, ny, batch), dz2, wb + LBM_CLOSURE_OFF_W2, nullptr, z1, nullptr, dz1, partial);
+        tc_grid(nx, ny, batch), dz2_map, wb + LBM_CLOSURE_OFF_W2, nullptr, z1, nullptr, dz1,
+        partial);
   } else {
     conv32_kernel<true><<<rows, kConv32Threads, kConv32Smem, s>>>(
         g, dz2, wb + LBM_CLOSURE_OFF_W2, nullptr, z1, nullptr, dz1, partial);
