@@ -795,6 +795,23 @@ def run_closure_forward(args) -> None:
     peak = peaks.get("bf16_tflops", 1590.0)
     achieved = flops / (ms * 1e-3) / 1e12
 
+    # One training step on the same batch: forward keeping the activations, loss, backward.
+    tb = cl.Buffers(nx, ny, B, train=True)
+    tb.x.copy_(bufs.x)
+    flags0 = torch.zeros((nx, ny), dtype=torch.int32, device="cuda")
+    target = torch.tensor(rng.normal(size=nx * ny * B).astype(np.float32), device="cuda")
+    for _ in range(W):
+        cl.forward(net, tb, stream)
+        cl.loss_and_grad(net, tb, target, flags0, stream)
+    e0.record()
+    for _ in range(K):
+        cl.forward(net, tb, stream)
+        cl.loss_and_grad(net, tb, target, flags0, stream)
+    e1.record()
+    e1.synchronize()
+    train_ms = e0.elapsed_time(e1) / K
+    del tb
+
     # The inference kernel: features + network + relaxation rates of one 1024x512 state, fused.
     rho = torch.tensor((1 + 0.01 * rng.normal(size=(nx, ny))).astype(np.float32), device="cuda")
     vel = torch.tensor((0.05 * rng.normal(size=(nx, ny, 2))).astype(np.float32), device="cuda")
@@ -828,10 +845,13 @@ def run_closure_forward(args) -> None:
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": None,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json bf16_tflops)",
-                     "kernel": "conv1_fwd + conv32_kernel (mma.sync) + conv3_fwd"},
+                     "kernel": "conv1_fwd + conv32_tc_kernel (tcgen05, TMEM) + conv3_fwd"},
         "fused_relaxation": {"ms": fused_ms, "tflops": fused_tf, "frac": fused_tf / peak,
                              "cells": nx * ny,
                              "kernel": "closure_fused_kernel (features + 3 layers + tau)"},
+        "training_step": {"ms": train_ms, "flops": 3 * flops,
+                          "tflops": 3 * flops / (train_ms * 1e-3) / 1e12,
+                          "what": "forward with activations kept + loss + backward (batch 8)"},
         "cpu_baseline": None,
         "e2e": None,
         "gpu_launches": 4 * K,
