@@ -715,6 +715,7 @@ def run_closure(args) -> None:
             "test_seed": cfg.test_seed,
             "snapshots": S,
             "fine_steps_judged": verdict.fine_steps,
+            "kernel_sources": __import__("boltzmann_b200.provenance").provenance.digest("closure"),
             "l2": "stencil inputs larger than L2 at the fine size; no flush",
         },
         "closure": summary,
@@ -841,7 +842,9 @@ def run_closure_forward(args) -> None:
         "data": "synthetic",
         "config": {"workload": "closure network forward, batch 8 x 1024x512, 3x3 conv "
                                "4->32->32->1", "flops_per_cell": 21_312,
-                   "l2": "activations 2 x 268 MB per pass exceed L2; no flush"},
+                   "l2": "activations 2 x 268 MB per pass exceed L2; no flush",
+                   "kernel_sources": __import__("boltzmann_b200.provenance").provenance.digest(
+                       "closure")},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": None,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json bf16_tflops)",
