@@ -53,7 +53,7 @@ StepArgs<Real> make_step_args(const lbm_sim& s, bool write_moments) {
   }
   a.ntracers = (int)s.tracers.size();
   for (int t = 0; t < a.ntracers; ++t) {
-    a.tr[t].g = static_cast<Real*>(s.tracers[t].g);
+    a.tr[t].g = s.tracers[t].g;
     a.tr[t].val = static_cast<Real*>(s.tracers[t].val);
     a.tr[t].omega = s.tracers[t].omega;
     a.tr[t].omega_neg = s.tracers[t].omega_neg;
@@ -79,9 +79,9 @@ void step_geometry(const StepArgs<Real>& a, dim3& grid, dim3& block) {
 // Ring depth of the TMA kernel: as many stages as fit in ~50 KB per CTA (2-4), so that three or
 // four CTAs (24-32 consumer warps) share an SM and each keeps one or more tiles of copies in
 // flight while it computes another.
-template <class L, int K, int NT, bool EVEN, bool WR>
+template <class L, int K, int NT, bool EVEN, bool WR, int KT = default_tracer_kind<K>()>
 constexpr int tma_stages() {
-  constexpr size_t b = TmaStage<L, K, NT, EVEN, WR>::bytes;
+  constexpr size_t b = TmaStage<L, K, NT, EVEN, WR, KT>::bytes;
   constexpr int s = (int)((50 * 1024) / b);
   return s < 2 ? 2 : (s > 4 ? 4 : s);
 }
@@ -143,16 +143,16 @@ bool encode_row_map(CUtensorMap* map, const void* base, long long rows, int nz) 
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <class L, bool TRT, int K, bool EVEN, int NT, bool WR>
+template <class L, bool TRT, int K, bool EVEN, int NT, bool WR, int KT>
 cudaError_t launch_tma(const StepArgs<typename Pop<K>::real>& a, cudaStream_t stream) {
-  constexpr int S = tma_stages<L, K, NT, EVEN, WR>();
-  constexpr size_t smem = tma_smem_bytes<L, K, NT, EVEN, S, WR>();
+  constexpr int S = tma_stages<L, K, NT, EVEN, WR, KT>();
+  constexpr size_t smem = tma_smem_bytes<L, K, NT, EVEN, S, WR, KT>();
   // Two cells a consumer thread: D3Q27 BGK with 16-bit populations and no tracer, on the steps
   // whose results go back through the stage. (TRT needs more than the 128 registers three CTAs
   // a SM leave a thread, and spills.)
   constexpr bool PAIR = L::Q >= 27 && !TRT && dev_in<K>() && NT == 0 && (!EVEN || WR);
   constexpr int threads = tma_threads<PAIR>();
-  auto kern = aa_tma_kernel<L, TRT, K, EVEN, NT, S, WR, PAIR>;
+  auto kern = aa_tma_kernel<L, TRT, K, EVEN, NT, S, WR, PAIR, KT>;
   static std::once_flag once;
   static cudaError_t setup_err = cudaSuccess;
   static int per_sm = 1;
@@ -178,14 +178,15 @@ cudaError_t launch_tma(const StepArgs<typename Pop<K>::real>& a, cudaStream_t st
     using Real = typename Pop<K>::real;
     bool ok = encode_slot_map<T>(&maps.f, a.f, a.n, L::Q);
     if constexpr (NT == 1)
-      ok = ok && encode_slot_map<Real>(&maps.g, a.tr[0].g, a.n, TracerLattice<L::D>::type::Q);
+      ok = ok && encode_slot_map<typename TracerPop<KT>::type>(&maps.g, a.tr[0].g, a.n,
+                                                              TracerLattice<L::D>::type::Q);
     maps.use = ok ? 1 : 0;
   }
   kern<<<(unsigned)grid, threads, smem, stream>>>(a, maps);
   return cudaGetLastError();
 }
 
-template <class L, bool TRT, int K, bool EVEN, int NT>
+template <class L, bool TRT, int K, bool EVEN, int NT, int KT = default_tracer_kind<K>()>
 cudaError_t launch_one(const StepArgs<typename Pop<K>::real>& a, cudaStream_t stream,
                        int64_t* launches) {
   // Rows that split into whole 256-cell tiles go through the TMA-staged kernel (fused tracers:
@@ -199,16 +200,16 @@ cudaError_t launch_one(const StepArgs<typename Pop<K>::real>& a, cudaStream_t st
     if (fits && staged) {
       cudaError_t e;
       if (EVEN && a.nz == kTmaTile)
-        e = launch_tma<L, TRT, K, EVEN, NT, EVEN>(a, stream);
+        e = launch_tma<L, TRT, K, EVEN, NT, EVEN, KT>(a, stream);
       else
-        e = launch_tma<L, TRT, K, EVEN, NT, false>(a, stream);
+        e = launch_tma<L, TRT, K, EVEN, NT, false, KT>(a, stream);
       if (e == cudaSuccess) ++launches[1];
       return e;
     }
   }
   dim3 grid, block;
   step_geometry(a, grid, block);
-  aa_step_kernel<L, TRT, K, EVEN, NT><<<grid, block, 0, stream>>>(a);
+  aa_step_kernel<L, TRT, K, EVEN, NT, KT><<<grid, block, 0, stream>>>(a);
   const cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) ++launches[0];
   return e;
@@ -219,14 +220,25 @@ cudaError_t launch_typed(const lbm_sim& s, bool even, bool write_moments) {
   using Real = typename Pop<K>::real;
   const StepArgs<Real> a = make_step_args<Real>(s, write_moments);
   // Fused tracers: none, exactly one (loads hoisted with the fluid's), or a runtime count.
+  // 16-bit tracer populations (the fluid's own 16-bit kind) take the one-tracer path only.
   const int nt = a.ntracers;
+  const bool t16 = s.tracer_storage == K && dev_in<K>();
+  if (t16 && nt > 1) return cudaErrorNotSupported;
   if (even) {
     if (nt == 0) return launch_one<L, TRT, K, true, 0>(a, s.stream, s.launches);
-    if (nt == 1) return launch_one<L, TRT, K, true, 1>(a, s.stream, s.launches);
+    if (nt == 1) {
+      if constexpr (dev_in<K>())
+        if (t16) return launch_one<L, TRT, K, true, 1, K>(a, s.stream, s.launches);
+      return launch_one<L, TRT, K, true, 1>(a, s.stream, s.launches);
+    }
     return launch_one<L, TRT, K, true, -1>(a, s.stream, s.launches);
   }
   if (nt == 0) return launch_one<L, TRT, K, false, 0>(a, s.stream, s.launches);
-  if (nt == 1) return launch_one<L, TRT, K, false, 1>(a, s.stream, s.launches);
+  if (nt == 1) {
+    if constexpr (dev_in<K>())
+      if (t16) return launch_one<L, TRT, K, false, 1, K>(a, s.stream, s.launches);
+    return launch_one<L, TRT, K, false, 1>(a, s.stream, s.launches);
+  }
   return launch_one<L, TRT, K, false, -1>(a, s.stream, s.launches);
 }
 

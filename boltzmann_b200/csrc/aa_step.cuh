@@ -37,7 +37,7 @@ constexpr int kMaxTracers = 4;
 
 template <class Real>
 struct TracerArgs {
-  Real* g;    // [Qt][N]
+  void* g;    // [Qt][N] in the tracer storage type (TracerPop)
   Real* val;  // [N]
   Real omega;      // omega (BGK) or omega+ (TRT)
   Real omega_neg;  // omega- (TRT)
@@ -395,7 +395,7 @@ __device__ __forceinline__ void tracer_update(const TracerArgs<Real>& tr, long l
     collide_packed<TL, false, false>(g, rt, rt, u, uu, om, om);
   else
     collide<TL, false, false>(g, rt, rt, u, uu, om, om);
-  sink.template tracer<TL, TP, EVEN>(tr.g, n, c, g);
+  sink.template tracer<TL, TP, EVEN>(static_cast<typename TP::type*>(tr.g), n, c, g);
   if (keep && !tfixed) tr.val[c.cell] = rt;
 }
 
@@ -425,7 +425,9 @@ __device__ __forceinline__ CellPos make_cellpos(const StepArgs<Real>& a, int x, 
 // (NT == 1), cval the coupled tracer's previous value.
 // om_pos / om_neg are the relaxation rates of the cell's domain (a.om_pos / a.om_neg for a single
 // simulation; per domain in an ensemble).
-template <class L, bool TRT, int K, bool EVEN, int NT, class Sink = GlobalSink>
+// KT: storage kind of the fused tracers' populations (TracerPop).
+template <class L, bool TRT, int K, bool EVEN, int NT, class Sink = GlobalSink,
+          int KT = default_tracer_kind<K>()>
 __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real>& a,
                                             const CellPos& c, int flag,
                                             typename Pop<K>::real (&f)[L::Q],
@@ -438,7 +440,7 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
   using Real = typename P::real;
   using T = typename P::type;
   using TL = typename TracerLattice<L::D>::type;
-  using TP = Pop<(sizeof(Real) == 8 ? kF64 : kF32)>;
+  using TP = TracerPop<KT>;
   constexpr int Q = L::Q;
 
   if (flag & 1) return;  // WALL: never updated (src/lib.cl:210-213)
@@ -524,7 +526,7 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
   } else if constexpr (NT < 0) {
     for (int t = 0; t < a.ntracers; ++t) {
       Real gt[TL::Q];
-      aa_load<TL, TP, EVEN, false>(a.tr[t].g, a.n, c, gt);
+      aa_load<TL, TP, EVEN, false>(static_cast<const typename TP::type*>(a.tr[t].g), a.n, c, gt);
       const bool keep = a.write_moments || (a.acc_mode == kAccBoussinesq && t == a.coupled);
       tracer_update<TL, TP, EVEN>(a.tr[t], a.n, c, flag, gt, u, uu, keep);
     }
@@ -535,14 +537,14 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
 // NT: number of fused tracers known at compile time (0 or 1), or -1 for a runtime count.
 // Every load a cell needs is issued before the first branch on any loaded value, so each thread
 // has one memory phase (walls load populations they then ignore; they are a small fraction).
-template <class L, bool TRT, int K, bool EVEN, int NT>
+template <class L, bool TRT, int K, bool EVEN, int NT, int KT = default_tracer_kind<K>()>
 __global__ void __launch_bounds__(256)
     aa_step_kernel(const __grid_constant__ StepArgs<typename Pop<K>::real> a) {
   using P = Pop<K>;
   using Real = typename P::real;
   using T = typename P::type;
   using TL = typename TracerLattice<L::D>::type;
-  using TP = Pop<(sizeof(Real) == 8 ? kF64 : kF32)>;
+  using TP = TracerPop<KT>;
 
   const int z = blockIdx.x * blockDim.x + threadIdx.x;
   if (z >= a.nz) return;
@@ -554,10 +556,12 @@ __global__ void __launch_bounds__(256)
       Real f[L::Q];
       aa_load<L, P, EVEN, dev_in<K>()>(static_cast<const T*>(a.f), a.n, c, f);
       Real g[NT == 1 ? TL::Q : 1];
-      if constexpr (NT == 1) aa_load<TL, TP, EVEN, false>(a.tr[0].g, a.n, c, g);
+      if constexpr (NT == 1)
+        aa_load<TL, TP, EVEN, false>(static_cast<const typename TP::type*>(a.tr[0].g), a.n, c, g);
       Real cval = 0;
       if (a.acc_mode == kAccBoussinesq) cval = a.coupled_val[c.cell];
-      update_cell<L, TRT, K, EVEN, NT>(a, c, flag, f, g, cval, a.om_pos, a.om_neg);
+      update_cell<L, TRT, K, EVEN, NT, GlobalSink, KT>(a, c, flag, f, g, cval, a.om_pos,
+                                                      a.om_neg);
     }
   }
 }

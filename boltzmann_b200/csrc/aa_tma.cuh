@@ -159,22 +159,24 @@ __device__ __forceinline__ void bulk_wait_all() {
 
 // Shared-memory layout of one stage, in elements of each operand's type.
 // WR: rows of one tile (even steps then copy whole rows and need no halo).
-template <class L, int K, int NT, bool EVEN, bool WR = false>
+template <class L, int K, int NT, bool EVEN, bool WR = false, int KT = default_tracer_kind<K>()>
 struct TmaStage {
   using T = typename Pop<K>::type;
   using Real = typename Pop<K>::real;
+  using TP = TracerPop<KT>;       // the fused tracer's population storage
+  using TT = typename TP::type;
   using TL = typename TracerLattice<L::D>::type;
   static constexpr int Q = L::Q;
   static constexpr int NG = NT == 1 ? TL::Q : 0;
   static constexpr int H = EVEN && !WR ? 16 / (int)sizeof(T) : 0;      // population halo
-  static constexpr int HG = EVEN && !WR ? 16 / (int)sizeof(Real) : 0;  // tracer halo
+  static constexpr int HG = EVEN && !WR ? 16 / (int)sizeof(TT) : 0;    // tracer halo
   static constexpr int SEG = kTmaTile + 2 * H;                   // populations per direction
   static constexpr int SEGG = kTmaTile + 2 * HG;
   // Even steps of one-tile rows move slots four rows at a time; the last group is padded with
   // repeats of slot Q - 1 into rows Q .. QP - 1 of the stage.
   static constexpr int QP = EVEN && WR ? 4 * ((Q + 3) / 4) : Q;
   static constexpr size_t pop_bytes = (size_t)QP * SEG * sizeof(T);
-  static constexpr size_t trc_bytes = (size_t)NG * SEGG * sizeof(Real);
+  static constexpr size_t trc_bytes = ((size_t)NG * SEGG * sizeof(TT) + 15) / 16 * 16;
   static constexpr size_t val_bytes = (size_t)kTmaTile * sizeof(Real);
   static constexpr size_t flag_bytes = kTmaTile;
   // offsets (bytes) inside a stage; every part 16-byte aligned, stages 128-byte aligned (the
@@ -185,9 +187,10 @@ struct TmaStage {
   static constexpr size_t bytes = (off_flag + flag_bytes + 127) / 128 * 128;
 };
 
-template <class L, int K, int NT, bool EVEN, int S, bool WR = false>
+template <class L, int K, int NT, bool EVEN, int S, bool WR = false,
+          int KT = default_tracer_kind<K>()>
 __host__ __device__ constexpr size_t tma_smem_bytes() {
-  return (size_t)S * TmaStage<L, K, NT, EVEN, WR>::bytes + 16 * S;  // + full/empty mbarriers
+  return (size_t)S * TmaStage<L, K, NT, EVEN, WR, KT>::bytes + 16 * S;  // + full/empty mbarriers
 }
 
 // Bulk-copies the row segment [z0 - hl, z0 + T + hr) of one operand row (elements of `es` bytes)
@@ -241,16 +244,16 @@ struct StageSink {
       for (int r = LL::Q; r < St::QP; ++r) base[r * St::SEG + pos] = w;
     }
   }
-  template <class TT, class TP, bool EVEN>
+  template <class TLL, class TP, bool EVEN>
   __device__ __forceinline__ void tracer(typename TP::type*, long long, const CellPos&,
-                                         const typename TP::real (&v)[TT::Q]) const {
-    using Real = typename TP::real;
-    Real* base = reinterpret_cast<Real*>(st + St::off_trc);
+                                         const typename TP::real (&v)[TLL::Q]) const {
+    using TT = typename TP::type;
+    TT* base = reinterpret_cast<TT*>(st + St::off_trc);
 #pragma unroll
-    for (int i = 0; i < TT::Q; ++i) {
-      Real* p = base + i * St::SEGG +
-                (EVEN ? St::HG + ((tid - comp<TT>(i, 2)) & (kTmaTile - 1)) : tid);
-      *p = EVEN ? v[opp(i)] : v[i];
+    for (int i = 0; i < TLL::Q; ++i) {
+      TT* p = base + i * St::SEGG +
+              (EVEN ? St::HG + ((tid - comp<TLL>(i, 2)) & (kTmaTile - 1)) : tid);
+      TP::store(p, EVEN ? v[opp(i)] : v[i], 0.0f);
     }
   }
 };
@@ -279,7 +282,8 @@ constexpr int tma_min_blocks() {
 }
 
 // Warp-specialised: warps 0..7 consume (one cell per thread), warp 8 loads and stores stages.
-template <class L, bool TRT, int K, bool EVEN, int NT, int S, bool WR, bool PAIR = false>
+template <class L, bool TRT, int K, bool EVEN, int NT, int S, bool WR, bool PAIR = false,
+          int KT = default_tracer_kind<K>()>
 __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR>())
     aa_tma_kernel(const __grid_constant__ StepArgs<typename Pop<K>::real> a,
                   const __grid_constant__ TmaMaps maps) {
@@ -287,7 +291,9 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
   using Real = typename P::real;
   using T = typename P::type;
   using TL = typename TracerLattice<L::D>::type;
-  using St = TmaStage<L, K, NT, EVEN, WR>;
+  using St = TmaStage<L, K, NT, EVEN, WR, KT>;
+  using TP = TracerPop<KT>;
+  using TT = typename TP::type;
   constexpr int Q = L::Q;
 
   extern __shared__ __align__(128) unsigned char smem[];
@@ -396,13 +402,13 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
           const int i = op - Q;
           const int slot = i;
           const int cz = EVEN && !whole_row ? comp_rt<TL, 2>(i) : 0;
-          jb.base = reinterpret_cast<const unsigned char*>(a.tr[0].g + (size_t)slot * a.n);
+          jb.base = static_cast<const unsigned char*>(a.tr[0].g) + (size_t)slot * a.n * sizeof(TT);
           jb.cx = EVEN ? comp_rt<TL, 0>(i) : 0;
           jb.cy = EVEN ? comp_rt<TL, 1>(i) : 0;
           jb.hl = cz > 0 ? St::HG : 0;
           jb.hr = cz < 0 ? St::HG : 0;
-          jb.es = sizeof(Real);
-          jb.dst = (unsigned)(St::off_trc + ((size_t)i * St::SEGG + St::HG - jb.hl) * sizeof(Real));
+          jb.es = sizeof(TT);
+          jb.dst = (unsigned)(St::off_trc + ((size_t)i * St::SEGG + St::HG - jb.hl) * sizeof(TT));
           jb.kind = 1;
         }
       } else if (op == Q + St::NG) {
@@ -618,10 +624,10 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
     if constexpr (NT == 1) {
 #pragma unroll
       for (int i = 0; i < St::NG; ++i) {
-        const Real* seg = reinterpret_cast<const Real*>(
-            st + St::off_trc + (size_t)(EVEN ? i : opp(i)) * St::SEGG * sizeof(Real));
+        const TT* seg = reinterpret_cast<const TT*>(
+            st + St::off_trc + (size_t)(EVEN ? i : opp(i)) * St::SEGG * sizeof(TT));
         const int zi = whole_row ? (tid - comp<TL>(i, 2)) & (kTmaTile - 1) : tid - comp<TL>(i, 2);
-        g[i] = EVEN ? seg[St::HG + zi] : seg[tid];
+        g[i] = TP::load(EVEN ? seg + St::HG + zi : seg + tid, 0.0f);
       }
     }
     const Real cval = a.acc_mode == kAccBoussinesq
@@ -632,12 +638,14 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
     if (!bulk_out) {
       __syncwarp();
       if (lane == 0) mbar_arrive(empty + s);  // this warp is done with stage s
-      update_cell<L, TRT, K, EVEN, NT>(a, c, flag, fv, g, cval, a.om_pos, a.om_neg);
+      update_cell<L, TRT, K, EVEN, NT, GlobalSink, KT>(a, c, flag, fv, g, cval, a.om_pos,
+                                                      a.om_neg);
       continue;
     }
     // Results into the stage, where the producer picks them up as whole row segments.
     const StageSink<St, L, TL> sink{const_cast<unsigned char*>(st), tid};
-    update_cell<L, TRT, K, EVEN, NT>(a, c, flag, fv, g, cval, a.om_pos, a.om_neg, sink);
+    update_cell<L, TRT, K, EVEN, NT, StageSink<St, L, TL>, KT>(a, c, flag, fv, g, cval, a.om_pos,
+                                                              a.om_neg, sink);
     fence_proxy_async();  // this thread's stage writes, visible to the bulk stores
     __syncwarp();
     if (lane == 0) mbar_arrive(empty + s);

@@ -215,7 +215,8 @@ int lbm_device_bytes(lbm_sim* sim, int64_t* out) {
   if (int rc = activate(sim)) return rc;
   const int64_t n = sim->n, rb = (int64_t)sim->real_bytes();
   int64_t b = n * sim->q * (int64_t)lbm::pop_bytes(sim->storage) + n * rb * (1 + sim->dim) + n;
-  for (const lbm_sim::Tracer& t : sim->tracers) b += n * rb * (t.q + 1);
+  for (const lbm_sim::Tracer& t : sim->tracers)
+    b += n * (int64_t)sim->tracer_pop_bytes() * t.q + n * rb;
   *out = b;
   return LBM_OK;
 }
@@ -234,18 +235,36 @@ int lbm_add_tracer(lbm_sim* sim, int q, int collision, float omega_pos, float om
   t.collision = collision;
   t.omega = omega_pos;
   t.omega_neg = omega_neg;
-  const size_t rb = sim->real_bytes();
-  LBM_CUDA(cudaMalloc(&t.g, (size_t)sim->n * q * rb));
+  if (sim->tracer_storage >= 0 && !sim->tracers.empty())
+    return fail(LBM_ERR_UNSUPPORTED, "16-bit tracer storage takes one tracer");
+  const size_t rb = sim->real_bytes(), gb = sim->tracer_pop_bytes();
+  LBM_CUDA(cudaMalloc(&t.g, (size_t)sim->n * q * gb));
   cudaError_t e = cudaMalloc(&t.val, (size_t)sim->n * rb);
   if (e != cudaSuccess) {
     cudaFree(t.g);
     return cuda_fail(e, "cudaMalloc(tracer val)");
   }
-  LBM_CUDA(cudaMemsetAsync(t.g, 0, (size_t)sim->n * q * rb, sim->stream));
+  LBM_CUDA(cudaMemsetAsync(t.g, 0, (size_t)sim->n * q * gb, sim->stream));
   LBM_CUDA(cudaMemsetAsync(t.val, 0, (size_t)sim->n * rb, sim->stream));
   sim->tracers.push_back(t);
   if (out_index) *out_index = (int)sim->tracers.size() - 1;
   return LBM_OK;
+}
+
+int lbm_set_tracer_storage(lbm_sim* sim, int storage) {
+  if (int rc = activate(sim)) return rc;
+  if (!sim->tracers.empty())
+    return fail(LBM_ERR_STATE, "the tracer storage is chosen before the first tracer is added");
+  if (storage == LBM_STORAGE_F32 && sim->storage != LBM_STORAGE_F64) {
+    sim->tracer_storage = -1;
+    return LBM_OK;
+  }
+  if ((storage == LBM_STORAGE_F16 || storage == LBM_STORAGE_BF16) && storage == sim->storage) {
+    sim->tracer_storage = storage;
+    return LBM_OK;
+  }
+  return fail(LBM_ERR_UNSUPPORTED,
+              "tracer populations are stored as float, or in the fluid's own 16-bit kind");
 }
 
 int lbm_set_gravity(lbm_sim* sim, const float* g) {
@@ -372,6 +391,8 @@ int lbm_iterate(lbm_sim* sim, int64_t iters) {
     const bool last = it == iters - 1;
     cudaError_t e = sim->dim == 2 ? lbm::launch_step_d2q9(*sim, even, last)
                                   : lbm::launch_step_d3q27(*sim, even, last);
+    if (e == cudaErrorNotSupported)
+      return fail(LBM_ERR_UNSUPPORTED, "16-bit tracer storage takes one tracer");
     if (e != cudaSuccess) return cuda_fail(e, "AA step launch");
   }
   return LBM_OK;

@@ -43,8 +43,9 @@ __device__ __forceinline__ double feq_f64(int i, double rho, const double* u) {
   return rho * L::wd(i) * (1.0 + 3.0 * vq + 4.5 * vq * vq - 1.5 * vv);
 }
 
-// f[i*n + cell] = feq_i(rho[cell], vel[cell]) for one velocity set L and storage K.
-template <class L, int K>
+// f[i*n + cell] = feq_i(rho[cell], vel[cell]) for one velocity set L and storage K (16-bit
+// kinds: the offset f_i - w_i; RAW: the value itself, for 16-bit tracer populations).
+template <class L, int K, bool RAW = false>
 __global__ void equilibrate_kernel(typename Pop<K>::type* __restrict__ f,
                                    const typename Pop<K>::real* __restrict__ rho,
                                    const typename Pop<K>::real* __restrict__ vel, int64_t n) {
@@ -63,44 +64,55 @@ __global__ void equilibrate_kernel(typename Pop<K>::type* __restrict__ f,
         fe = feq_f64<L>(i, r, u);
       else
         fe = feq_f32<L>(i, r, u);
-      P::store(f + (int64_t)i * n + cell, fe, weight<L, Real>(i));
+      P::store(f + (int64_t)i * n + cell, fe, RAW ? Real(0) : weight<L, Real>(i));
     }
   }
 }
 
-template <class L, int K>
+template <class L, int K, bool RAW>
 cudaError_t equilibrate_set(void* f, const void* rho, const void* vel, int64_t n, cudaStream_t s) {
   using P = Pop<K>;
-  equilibrate_kernel<L, K><<<blocks_for(n), kThreads, 0, s>>>(
+  equilibrate_kernel<L, K, RAW><<<blocks_for(n), kThreads, 0, s>>>(
       static_cast<typename P::type*>(f), static_cast<const typename P::real*>(rho),
       static_cast<const typename P::real*>(vel), n);
   return cudaGetLastError();
 }
 
-template <class L>
+template <class L, bool RAW>
 cudaError_t equilibrate_storage(int storage, void* f, const void* rho, const void* vel, int64_t n,
                                 cudaStream_t s) {
   switch (storage) {
-    case kF32: return equilibrate_set<L, kF32>(f, rho, vel, n, s);
-    case kF16: return equilibrate_set<L, kF16>(f, rho, vel, n, s);
-    case kBF16: return equilibrate_set<L, kBF16>(f, rho, vel, n, s);
-    case kF64: return equilibrate_set<L, kF64>(f, rho, vel, n, s);
+    case kF32: return equilibrate_set<L, kF32, false>(f, rho, vel, n, s);
+    case kF16: return equilibrate_set<L, kF16, RAW>(f, rho, vel, n, s);
+    case kBF16: return equilibrate_set<L, kBF16, RAW>(f, rho, vel, n, s);
+    case kF64: return equilibrate_set<L, kF64, false>(f, rho, vel, n, s);
   }
   return cudaErrorInvalidValue;
 }
 
-// `storage` is the storage kind of the buffer f (the fluid's kind, or F32/F64 for tracers).
+// `storage` is the storage kind of the buffer f (the fluid's kind, or the tracers'); `raw`: a
+// 16-bit buffer holds the values themselves (tracer populations), not offsets from the weights.
 cudaError_t equilibrate_any(int d, int q, int storage, void* f, const void* rho, const void* vel,
-                            int64_t n, cudaStream_t s) {
-  if (d == 1 && q == 3) return equilibrate_storage<D1Q3>(storage, f, rho, vel, n, s);
-  if (d == 2 && q == 9) return equilibrate_storage<D2Q9>(storage, f, rho, vel, n, s);
-  if (d == 2 && q == 5) return equilibrate_storage<D2Q5>(storage, f, rho, vel, n, s);
-  if (d == 3 && q == 7) return equilibrate_storage<D3Q7>(storage, f, rho, vel, n, s);
-  if (d == 3 && q == 27) return equilibrate_storage<D3Q27>(storage, f, rho, vel, n, s);
+                            int64_t n, cudaStream_t s, bool raw = false) {
+  if (raw) {
+    if (d == 2 && q == 5) return equilibrate_storage<D2Q5, true>(storage, f, rho, vel, n, s);
+    if (d == 3 && q == 7) return equilibrate_storage<D3Q7, true>(storage, f, rho, vel, n, s);
+    return cudaErrorNotSupported;
+  }
+  if (d == 1 && q == 3) return equilibrate_storage<D1Q3, false>(storage, f, rho, vel, n, s);
+  if (d == 2 && q == 9) return equilibrate_storage<D2Q9, false>(storage, f, rho, vel, n, s);
+  if (d == 2 && q == 5) return equilibrate_storage<D2Q5, false>(storage, f, rho, vel, n, s);
+  if (d == 3 && q == 7) return equilibrate_storage<D3Q7, false>(storage, f, rho, vel, n, s);
+  if (d == 3 && q == 27) return equilibrate_storage<D3Q27, false>(storage, f, rho, vel, n, s);
   return cudaErrorNotSupported;
 }
 
-inline int tracer_storage(const lbm_sim& sim) { return sim.storage == kF64 ? kF64 : kF32; }
+inline int tracer_storage(const lbm_sim& sim) { return sim.tracer_kind(); }
+// 16-bit tracer populations are stored as values, so their layout transposes and sums take zero
+// offsets.
+inline bool tracer_raw(const lbm_sim& sim) {
+  return sim.tracer_kind() == kF16 || sim.tracer_kind() == kBF16;
+}
 
 // Per-slot weights of any velocity set, for the offset encodings of the layout transposes.
 struct SlotWeights {
@@ -241,7 +253,8 @@ cudaError_t equilibrate(const lbm_sim& sim) {
                                   sim.stream);
   if (e != cudaSuccess) return e;
   for (const lbm_sim::Tracer& t : sim.tracers) {
-    e = equilibrate_any(sim.dim, t.q, tracer_storage(sim), t.g, t.val, sim.vel, sim.n, sim.stream);
+    e = equilibrate_any(sim.dim, t.q, tracer_storage(sim), t.g, t.val, sim.vel, sim.n, sim.stream,
+                        tracer_raw(sim));
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -250,7 +263,7 @@ cudaError_t equilibrate(const lbm_sim& sim) {
 cudaError_t equilibrate_tracer(const lbm_sim& sim, int tracer) {
   const lbm_sim::Tracer& t = sim.tracers[tracer];
   return equilibrate_any(sim.dim, t.q, tracer_storage(sim), t.g, t.val, sim.vel, sim.n,
-                         sim.stream);
+                         sim.stream, tracer_raw(sim));
 }
 
 cudaError_t populations_from_aos(const lbm_sim& sim, int tracer, const float* d_aos) {
@@ -262,6 +275,7 @@ cudaError_t populations_from_aos(const lbm_sim& sim, int tracer, const float* d_
   }
   const lbm_sim::Tracer& t = sim.tracers[tracer];
   if (!weights_for(sim.dim, t.q, sw)) return cudaErrorNotSupported;
+  if (tracer_raw(sim)) sw = SlotWeights{};
   return transpose<true>(tracer_storage(sim), t.g, const_cast<float*>(d_aos), sim.n,
                          t.q, sw, sim.stream);
 }
@@ -274,6 +288,7 @@ cudaError_t populations_to_aos(const lbm_sim& sim, int tracer, float* d_aos) {
   }
   const lbm_sim::Tracer& t = sim.tracers[tracer];
   if (!weights_for(sim.dim, t.q, sw)) return cudaErrorNotSupported;
+  if (tracer_raw(sim)) sw = SlotWeights{};
   return transpose<false>(tracer_storage(sim), t.g, d_aos, sim.n, t.q, sw,
                           sim.stream);
 }
@@ -310,6 +325,8 @@ cudaError_t conservation_sums(const lbm_sim& sim, double* d_out) {
   for (size_t t = 0; t < sim.tracers.size(); ++t) {
     const lbm_sim::Tracer& tr = sim.tracers[t];
     if (!weights_for(sim.dim, tr.q, sw)) return cudaErrorNotSupported;
+    if (tracer_raw(sim))
+      for (int i = 0; i < 27; ++i) sw.w[i] = 0.0f;  // values, not offsets (the c_i stay)
     e = sums(tracer_storage(sim), tr.g, sim.n, tr.q, sim.dim, sw,
              d_out + 1 + sim.dim + t, 1, sim.stream);
     if (e != cudaSuccess) return e;

@@ -389,13 +389,18 @@ PYBIND11_MODULE(boltzmann, m) {
                          "Domain, fluid and tracers of one lattice-Boltzmann simulation "
                          "(src/lib.rs:171-399).")
       .def(py::init([](const std::string& dev, const std::vector<int64_t>& counts,
-                       const Omega& omega, std::optional<int> q, const std::string& storage) {
+                       const Omega& omega, std::optional<int> q, const std::string& storage,
+                       std::optional<std::string> tracer_storage) {
              check_device(dev);
              const int qq = q ? *q : default_q((int)counts.size(), false);
-             return Simulation{make_state(counts, omega, qq, parse_storage(storage))};
+             Simulation sim{make_state(counts, omega, qq, parse_storage(storage))};
+             // Tracer populations: float by default, or the fluid's own 16-bit kind.
+             if (tracer_storage)
+               check(lbm_set_tracer_storage(sim.st->h, parse_storage(*tracer_storage)));
+             return sim;
            }),
            py::arg("dev"), py::arg("counts"), py::arg("omega"), py::arg("q") = py::none(),
-           py::arg("storage") = "f32")
+           py::arg("storage") = "f32", py::arg("tracer_storage") = py::none())
       .def_property_readonly("device_info",
                              [](const Simulation& s) {
                                char buf[256] = {0};

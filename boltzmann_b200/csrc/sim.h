@@ -23,6 +23,9 @@ struct lbm_sim {
   };
 
   int dim = 0, q = 0, collision = 0, storage = 0;
+  // Storage kind of the tracers' populations: -1 for the fluid's compute type (float, double
+  // for FP64 runs), or the fluid's 16-bit kind (lbm_set_tracer_storage).
+  int tracer_storage = -1;
   int64_t counts[3] = {1, 1, 1};
   int64_t n = 0;  // cell count
   float om_pos = 0, om_neg = 0;
@@ -48,6 +51,9 @@ struct lbm_sim {
   std::vector<Coupling> couplings;
 
   size_t real_bytes() const { return storage == 3 ? 8 : 4; }
+  // Storage kind and element bytes of tracer populations.
+  int tracer_kind() const { return tracer_storage >= 0 ? tracer_storage : (storage == 3 ? 3 : 0); }
+  size_t tracer_pop_bytes() const { return tracer_kind() == 3 ? 8 : (tracer_kind() == 0 ? 4 : 2); }
 };
 
 namespace lbm {

@@ -76,6 +76,39 @@ struct Pop<kF64> {
   __device__ __forceinline__ static void store_dev(type* p, real d, real w) { *p = w + d; }
 };
 
+// Storage of tracer populations: the compute type (float, or double for FP64 runs), or 16-bit
+// values stored as they are -- a concentration spans 0 .. 1, so no fixed offset shrinks the stored
+// magnitudes -- widened to float for the update and rounded to nearest on store. The weight
+// argument is ignored (it is the fluid policies' offset).
+template <int KT>
+struct TracerPop;
+template <>
+struct TracerPop<kF32> : Pop<kF32> {};
+template <>
+struct TracerPop<kF64> : Pop<kF64> {};
+template <>
+struct TracerPop<kF16> {
+  using type = __half;
+  using real = float;
+  __device__ __forceinline__ static real load(const type* p, real) { return __half2float(*p); }
+  __device__ __forceinline__ static void store(type* p, real v, real) { *p = __float2half_rn(v); }
+};
+template <>
+struct TracerPop<kBF16> {
+  using type = __nv_bfloat16;
+  using real = float;
+  __device__ __forceinline__ static real load(const type* p, real) { return __bfloat162float(*p); }
+  __device__ __forceinline__ static void store(type* p, real v, real) {
+    *p = __float2bfloat16_rn(v);
+  }
+};
+
+// Tracer storage when none is chosen: the fluid's compute type.
+template <int K>
+__host__ __device__ constexpr int default_tracer_kind() {
+  return K == kF64 ? kF64 : kF32;
+}
+
 // 16-bit kinds store deviations f_i - W_i; the update takes them as loaded, without forming the
 // full values (their rounding, ~1e-3 relative, dwarfs any FP32 ordering effect). FP32 and FP64
 // load full values, whose momentum sum is the reference's.

@@ -93,6 +93,14 @@ LBM_API int lbm_device_bytes(lbm_sim* sim, int64_t* out);
 LBM_API int lbm_add_tracer(lbm_sim* sim, int q, int collision, float omega_pos, float omega_neg,
                    int* out_index);
 
+/* Storage of the tracers' populations, chosen before the first tracer is added: LBM_STORAGE_F32
+ * (the default; double for an LBM_STORAGE_F64 simulation) or the fluid's own 16-bit kind
+ * (LBM_STORAGE_F16 / _BF16 for a simulation created with it), which halves the tracer's bytes per
+ * cell update; 16-bit tracer populations hold the values themselves (not offsets) and take one
+ * tracer per simulation (LBM_ERR_UNSUPPORTED otherwise). The tracer values (val) stay float. No
+ * reference counterpart (the reference stores float). */
+LBM_API int lbm_set_tracer_storage(lbm_sim* sim, int storage);
+
 /* Constant body force, dim floats (src/simulation.rs:194-196). */
 LBM_API int lbm_set_gravity(lbm_sim* sim, const float* g);
 

@@ -64,6 +64,10 @@ class CApiSim:
         self.tq.append(tq)
         return idx.value
 
+    def set_tracer_storage(self, storage: str) -> int:
+        """lbm_set_tracer_storage; returns the status (0 on success)."""
+        return _lib.lbm_set_tracer_storage(self.h, STORAGE[storage])
+
     def set_gravity(self, g) -> None:
         g = np.ascontiguousarray(g, np.float32)
         check(_lib.lbm_set_gravity(self.h, _ptr(g)))
