@@ -67,14 +67,15 @@ def make_setup(workload: str, size: int | None = None):
     raise SystemExit(f"unknown workload {workload}")
 
 
-def algorithmic_bytes_per_cell(setup, storage: str) -> float:
+def algorithmic_bytes_per_cell(setup, storage: str, tracer_storage: str | None = None) -> float:
     """Population bytes read + written per cell update (+ the coupled tracer value, read and
     written every step). Flags and the end-of-call rho/vel writes are not counted."""
     q = 9 if len(setup.counts) == 2 else 27
     qt = 5 if len(setup.counts) == 2 else 7
     pop = {"f32": 4, "f16": 2, "bf16": 2, "f64": 8}[storage]
     real = 8 if storage == "f64" else 4
-    b = 2 * q * pop + len(setup.tracers) * 2 * qt * real
+    tpop = {"f16": 2, "bf16": 2}.get(tracer_storage or "", real)
+    b = 2 * q * pop + len(setup.tracers) * 2 * qt * tpop
     if setup.couplings:
         b += 2 * real
     return float(b)
@@ -183,12 +184,12 @@ def omega_for(kind: str, tau: float, tau_neg: float | None = None):
     return bgk(tau) if kind == "bgk" else trt(tau, tau_neg)
 
 
-def build_sim(setup, storage: str):
+def build_sim(setup, storage: str, tracer_storage: str | None = None):
     from boltzmann_b200 import workloads
     from boltzmann_b200.core import Simulation
 
     sim = Simulation("gpu", setup.counts, omega_for(setup.collision, setup.tau, setup.tau_neg),
-                     storage=storage)
+                     storage=storage, tracer_storage=tracer_storage)
     workloads.apply(sim, setup, omega_for)
     return sim
 
@@ -296,17 +297,24 @@ def config_block(setup, storage: str, world: int) -> dict:
     }
 
 
-def velocity_l2_vs_f64(setup, vel, lbm_steps: int) -> dict:
+def velocity_l2_vs_f64(setup, vel, lbm_steps: int, tracer=None) -> dict:
     """Relative velocity L2 error ||u - u64|| / ||u64|| of a run's final field against an FP64 run
-    of the same set-up on the GPU for the same number of steps (outside any timed region)."""
+    of the same set-up on the GPU for the same number of steps (outside any timed region); with a
+    tracer, its value's error as well."""
     sim = build_sim(setup, "f64")
     sim.iterate(lbm_steps)
     _, vel64 = sim._fluid_f64()
+    c64 = None
+    if tracer is not None:
+        c64 = np.array(sim.get_tracer(setup.tracers[0][0]).val, np.float64)
     del sim
-    v = np.asarray(vel, np.float64)
-    err = float(np.linalg.norm((v - vel64).ravel()) / np.linalg.norm(vel64.ravel()))
-    return {"value": err, "lbm_steps": lbm_steps, "field": "velocity",
-            "norm": "relative L2 over all cells", "against": "FP64 run on the GPU (same set-up)"}
+    rel = lambda a, b: float(np.linalg.norm((np.asarray(a, np.float64) - b).ravel())
+                             / np.linalg.norm(b.ravel()))
+    out = {"value": rel(vel, vel64), "lbm_steps": lbm_steps, "field": "velocity",
+           "norm": "relative L2 over all cells", "against": "FP64 run on the GPU (same set-up)"}
+    if tracer is not None:
+        out["tracer"] = rel(tracer, c64)
+    return out
 
 
 def run_ours(args) -> None:
@@ -323,7 +331,7 @@ def run_ours(args) -> None:
     K, W = args.steps, max(args.warmup, 3)
 
     # Device-timed run: inputs resident in HBM, only the AA kernels in the timed region.
-    sim = build_sim(setup, args.storage)
+    sim = build_sim(setup, args.storage, args.tracer_storage)
     sim.iterate(2 * W)  # upload, equilibrate, warm-up steps
     stream = torch.cuda.ExternalStream(sim._stream())
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -345,6 +353,8 @@ def run_ours(args) -> None:
     sim.iterate(2)  # read back; checks the state is still finite
     finite = bool(np.isfinite(sim.fluid.rho).all())
     final_vel = np.array(sim.fluid.vel, copy=True)
+    final_c = (np.array(sim.get_tracer(setup.tracers[0][0]).val, copy=True)
+               if setup.tracers else None)
     total_steps = sim.iteration
     del sim
     # The kernels the library launched in the timed region, from its own counters.
@@ -356,16 +366,19 @@ def run_ours(args) -> None:
 
     l2 = None
     if args.storage != "f64" and not args.no_l2:
-        l2 = velocity_l2_vs_f64(setup, final_vel, total_steps)
+        l2 = velocity_l2_vs_f64(setup, final_vel, total_steps, final_c)
 
     lbm_steps = 2 * K
     value = world * setup.cells * lbm_steps / (elapsed_ms * 1e-3) / 1e6
     launch_ms = elapsed_ms / lbm_steps
-    bpc = algorithmic_bytes_per_cell(setup, args.storage)
+    bpc = algorithmic_bytes_per_cell(setup, args.storage, args.tracer_storage)
     peaks, peak_kind = measured_peaks()
     achieved = bpc * setup.cells / (launch_ms * 1e-3) / 1e9
     tag = {"cylinder_channel": "d2q9_trt_tracer", "kelvin_helmholtz": "d2q9_bgk",
-           "taylor_green_3d": "d3q27_bgk"}[args.workload] + f"_{args.storage}"
+           "taylor_green_3d": "d3q27_bgk"}[args.workload]
+    if args.tracer_storage in ("f16", "bf16") and setup.tracers:
+        tag += "16"
+    tag += f"_{args.storage}"
     traffic_pc, traffic_src = profiled_traffic(f"{kernel}_{tag}", "stencil")
 
     # End to end through the public API with host buffers: a fresh Simulation from host arrays;
@@ -379,7 +392,7 @@ def run_ours(args) -> None:
     if not args.no_e2e:
         # Three fresh simulations, each timed over its one iterate call; the median is reported.
         for _ in range(3):
-            sim2 = build_sim(setup, args.storage)
+            sim2 = build_sim(setup, args.storage, args.tracer_storage)
             barrier()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -409,7 +422,9 @@ def run_ours(args) -> None:
             "dtype": {"f32": "f32", "f16": "f16-offset storage, f32 compute",
                       "bf16": "bf16-offset storage, f32 compute", "f64": "f64"}[args.storage],
             "data": "synthetic",
-            "config": config_block(setup, args.storage, world),
+            "config": dict(config_block(setup, args.storage, world),
+                           tracer_storage=args.tracer_storage or
+                           ("f64" if args.storage == "f64" else "f32")),
             "roofline": {
                 "bound": "hbm",
                 "achieved": achieved,
@@ -874,6 +889,8 @@ def main() -> None:
                     choices=["cylinder_channel", "kelvin_helmholtz", "taylor_green_3d",
                              "cavity_ensemble", "closure", "closure_forward"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f64"])
+    ap.add_argument("--tracer-storage", default=None, choices=["f16", "bf16"],
+                    help="store the fused tracer's populations in the fluid's 16-bit kind")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-l2", action="store_true",
