@@ -147,10 +147,12 @@ template <class L, bool TRT, int K, bool EVEN, int NT, bool WR, int KT>
 cudaError_t launch_tma(const StepArgs<typename Pop<K>::real>& a, cudaStream_t stream) {
   constexpr int S = tma_stages<L, K, NT, EVEN, WR, KT>();
   constexpr size_t smem = tma_smem_bytes<L, K, NT, EVEN, S, WR, KT>();
-  // Two cells a consumer thread: D3Q27 BGK with 16-bit populations and no tracer, on the steps
-  // whose results go back through the stage. (TRT needs more than the 128 registers three CTAs
-  // a SM leave a thread, and spills.)
-  constexpr bool PAIR = L::Q >= 27 && !TRT && dev_in<K>() && NT == 0 && (!EVEN || WR);
+  // Two cells a consumer thread with 16-bit populations: D3Q27 BGK without a tracer, on the
+  // steps whose results go back through the stage (D3Q27 TRT needs more than the 128 registers
+  // three CTAs a SM leave a thread, and spills); D2Q9 BGK / TRT with none or one fused tracer, on
+  // every step.
+  constexpr bool PAIR = dev_in<K>() && ((L::Q >= 27 && !TRT && NT == 0 && (!EVEN || WR)) ||
+                                        (L::D == 2 && NT >= 0 && NT <= 1));
   constexpr int threads = tma_threads<PAIR>();
   auto kern = aa_tma_kernel<L, TRT, K, EVEN, NT, S, WR, PAIR, KT>;
   static std::once_flag once;

@@ -219,6 +219,11 @@ __device__ __forceinline__ void collide(Real (&v)[L::Q], Real r, Real dr, const 
 // on packed instructions and must round identically).
 __device__ __forceinline__ float fma_r(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double fma_r(double a, double b, double c) { return fma(a, b, c); }
+// A product and a sum that are never contracted into a fused multiply-add.
+__device__ __forceinline__ float mul_r(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_r(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_r(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_r(double a, double b) { return __dadd_rn(a, b); }
 
 // ---- Packed FP32 (Blackwell FADD2 / FMUL2 / FFMA2): two independent FP32 operations per
 // instruction, each lane rounded exactly as the scalar operation (round to nearest even).
@@ -310,13 +315,14 @@ __device__ __forceinline__ void collide_packed(float (&v)[L::Q], float r, float 
   }
 }
 
-// Whether the collision of lattice L runs on packed FP32 pairs: D3Q27 (13 pairs, +5% MLUPS on
-// the 256^3 Taylor-Green run). For D2Q9 and the tracers the packed and scalar collisions
-// measured within 2% of each other (the D2Q9 kernels sit at their register cap), and scalar
-// was ahead with 16-bit storage.
-template <class L>
+// Whether the FP32 collision of lattice L (fluid or tracer) runs on packed pairs, with storage
+// kind K of the fluid: D3Q27 (13 pairs, +5% MLUPS on the 256^3 Taylor-Green run), and every
+// lattice of a simulation with 16-bit populations, whose staged kernels update two cells a
+// thread and must round as this one-cell path does (aa_pair.cuh). With FP32 storage the packed
+// and scalar D2Q9 / tracer collisions measured within 2% of each other.
+template <class L, int K>
 __host__ __device__ constexpr bool pack_collide() {
-  return L::Q >= 27;
+  return L::Q >= 27 || dev_in<K>();
 }
 
 // Moments of one cell for FP32. In: v full values (or deviations when DL). Out: v deviations,
@@ -374,7 +380,7 @@ __device__ __forceinline__ void moments_packed(float (&v)[L::Q], float& dr, floa
 // (src/lib.cl:102-189, 303-405), with its populations already loaded into g. TRT tracers take
 // the pair update of the fluid's TRT with their own rates, both 1 on fixed-value cells (the
 // D2Q5 / D3Q7 TRT kernels of python/boltzmann/kernel_gen.py:368-421).
-template <class TL, class TP, bool EVEN, class Real, class Sink = GlobalSink>
+template <class TL, class TP, bool EVEN, bool PACK, class Real, class Sink = GlobalSink>
 __device__ __forceinline__ void tracer_update(const TracerArgs<Real>& tr, long long n,
                                               const CellPos& c, int flag, Real (&g)[TL::Q],
                                               const Real (&u)[3], Real uu, bool keep,
@@ -389,12 +395,17 @@ __device__ __forceinline__ void tracer_update(const TracerArgs<Real>& tr, long l
     om_n = 1;
     rt = tr.val[c.cell];
   }
-  if (tr.trt)
-    collide<TL, true, false>(g, rt, rt, u, uu, om, om_n);
-  else if constexpr (sizeof(Real) == 4 && pack_collide<TL>())
-    collide_packed<TL, false, false>(g, rt, rt, u, uu, om, om);
-  else
-    collide<TL, false, false>(g, rt, rt, u, uu, om, om);
+  if constexpr (sizeof(Real) == 4 && PACK) {
+    if (tr.trt)
+      collide_packed<TL, true, false>(g, rt, rt, u, uu, om, om_n);
+    else
+      collide_packed<TL, false, false>(g, rt, rt, u, uu, om, om);
+  } else {
+    if (tr.trt)
+      collide<TL, true, false>(g, rt, rt, u, uu, om, om_n);
+    else
+      collide<TL, false, false>(g, rt, rt, u, uu, om, om);
+  }
   sink.template tracer<TL, TP, EVEN>(static_cast<typename TP::type*>(tr.g), n, c, g);
   if (keep && !tfixed) tr.val[c.cell] = rt;
 }
@@ -477,7 +488,7 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
   if constexpr (DL) {
     const Real rinv = __frcp_rn(r);  // one correctly rounded reciprocal; u within 1.5 ulp
 #pragma unroll
-    for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] *= rinv;
+    for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] = mul_r(u[ax], rinv);
   } else {
 #pragma unroll
     for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] = u[ax] / r;
@@ -488,7 +499,7 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
   // Force as a velocity shift acc / omega (src/lib.cl:253-256; TRT: omega+, 682-685).
   if (a.acc_mode == kAccConstant) {
 #pragma unroll
-    for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] += a.force[ax];
+    for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] = add_r(u[ax], a.force[ax]);
   } else if (a.acc_mode == kAccBoussinesq) {
     const Real b = a.alpha * (cval - a.c0);  // src/lib.cl:71
 #pragma unroll
@@ -507,7 +518,7 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
 #pragma unroll
   for (int ax = 4 - L::D; ax < 3; ++ax) uu = fma_r(u[ax], u[ax], uu);
 
-  if constexpr (sizeof(Real) == 4 && pack_collide<L>())
+  if constexpr (sizeof(Real) == 4 && pack_collide<L, K>())
     collide_packed<L, TRT, true>(f, r, dr, u, uu, om_pos, om_neg);
   else
     collide<L, TRT, true>(f, r, dr, u, uu, om_pos, om_neg);
@@ -522,13 +533,14 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
 
   if constexpr (NT == 1) {
     const bool keep = a.write_moments || (a.acc_mode == kAccBoussinesq && a.coupled == 0);
-    tracer_update<TL, TP, EVEN>(a.tr[0], a.n, c, flag, g, u, uu, keep, sink);
+    tracer_update<TL, TP, EVEN, pack_collide<TL, K>()>(a.tr[0], a.n, c, flag, g, u, uu, keep,
+                                                        sink);
   } else if constexpr (NT < 0) {
     for (int t = 0; t < a.ntracers; ++t) {
       Real gt[TL::Q];
       aa_load<TL, TP, EVEN, false>(static_cast<const typename TP::type*>(a.tr[t].g), a.n, c, gt);
       const bool keep = a.write_moments || (a.acc_mode == kAccBoussinesq && t == a.coupled);
-      tracer_update<TL, TP, EVEN>(a.tr[t], a.n, c, flag, gt, u, uu, keep);
+      tracer_update<TL, TP, EVEN, pack_collide<TL, K>()>(a.tr[t], a.n, c, flag, gt, u, uu, keep);
     }
   }
 }

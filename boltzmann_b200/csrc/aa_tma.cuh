@@ -11,10 +11,13 @@
 // when a row is a single tile the plain row is copied and the index wraps in shared memory) --
 // plus the fused tracer's populations, the coupled tracer value and the flag bytes.
 // Threads read their operands from shared memory (consecutive threads, consecutive words: no
-// bank conflicts) and collide. Odd steps, and even steps whose rows are one tile, write their
-// results back into the stage slot they came from, and the producer warp writes the stage back
-// with one bulk store per row segment (cp.async.bulk shared -> global) before refilling it.
-// Other even steps store straight to HBM with coalesced stores.
+// bank conflicts), collide, and write their results back into the stage at the positions they
+// read; the producer warp writes the stage back with one bulk store per row segment
+// (cp.async.bulk shared -> global) before refilling it. Even steps on rows longer than one tile
+// have shifted segments: there the bulk store takes the segment's 16-byte chunks and the cells
+// at the tile's ends store the few results outside them (edge_range).
+// 16-bit populations: two cells a consumer thread on packed FP32 instructions (aa_pair.cuh) for
+// D3Q27 BGK without a tracer and for D2Q9.
 //
 // In-flight data is bounded by shared memory, not by registers, and the copy engine issues one
 // instruction per row segment instead of one per element. Odd steps, which read their own row of
@@ -22,9 +25,8 @@
 // 256 cells by Q slots) when the launcher provides the maps.
 //
 // Synchronisation: stage s has a `full` mbarrier (the producer's expect_tx plus the copies'
-// bytes) and an `empty` one (one arrival per consumer warp: once its operands are in registers,
-// or, when results go back through the stage, once they are written there). Before refilling
-// stage s the producer waits on `empty`, issues the stage's bulk stores if it holds results and
+// bytes) and an `empty` one (one arrival per consumer warp, once its results are in the stage).
+// Before refilling stage s the producer waits on `empty`, issues the stage's bulk stores and
 // waits until they have read it. There is no CTA-wide barrier in the loop. Every wait is
 // bounded: on timeout the kernel sets bit 1 (value 2) of the status word and leaves.
 // Every population slot is still read and written by exactly one thread per step, and no tile
@@ -35,7 +37,6 @@
 
 #include <cstdint>
 
-#include "aa_pair.cuh"
 #include "aa_step.cuh"
 
 namespace lbm {
@@ -167,6 +168,7 @@ struct TmaStage {
   using TT = typename TP::type;
   using TL = typename TracerLattice<L::D>::type;
   static constexpr int Q = L::Q;
+  static constexpr bool kWR = WR;
   static constexpr int NG = NT == 1 ? TL::Q : 0;
   static constexpr int H = EVEN && !WR ? 16 / (int)sizeof(T) : 0;      // population halo
   static constexpr int HG = EVEN && !WR ? 16 / (int)sizeof(TT) : 0;    // tracer halo
@@ -211,23 +213,87 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// Index, inside its stage segment, of the population column `tid` reads and writes: its own
+// column on odd steps; on even steps the upstream column tid - cz behind the segment's halo h,
+// wrapped instead when rows are one tile (WR, no halo).
+template <bool WR, bool EVEN>
+__device__ __forceinline__ int stage_pos(int h, int tid, int cz) {
+  if constexpr (!EVEN) return tid;
+  if constexpr (WR) return (tid - cz) & (kTmaTile - 1);
+  return h + tid - cz;
+}
+
+// Even steps of rows longer than one tile read slot i of their tile's cells from the row
+// segment [z0 - c_iz, z0 - c_iz + 256) of the row upstream of c_i and write the results back to
+// the same positions. The stage holds element z0 - h + k of the segment at index k (h = 16 bytes
+// of elements, the halo), so the results are indices [h - c_iz, h - c_iz + 256): the producer
+// stores the 16-byte chunks wholly inside that range with one bulk store, and the h elements
+// left at its two ends (1 and h - 1, for c_iz != 0) come from the cells at the tile's ends.
+struct EdgeRange {
+  int first, last1;  // chunks [first, last1) of h elements lie wholly inside the result range
+};
+__host__ __device__ constexpr EdgeRange edge_range(int h, int cz) {
+  return EdgeRange{(h - cz + h - 1) / h, (h - cz + kTmaTile) / h};
+}
+
+// Whether column tid's result for a slot with z-component cz falls outside the bulk-stored chunks.
+__device__ __forceinline__ bool is_edge(int h, int tid, int cz) {
+  const EdgeRange r = edge_range(h, cz);
+  const int k = h + tid - cz;
+  return k < r.first * h || k >= r.last1 * h;
+}
+
+// The results of one cell at a tile's end (column col, neighbourhood e) that fall outside the
+// bulk-stored chunks, straight from its registers: fval(i) / gval(i) are its post-collision
+// populations and first tracer's (stored as in the stage: deviations for the populations).
+template <class St, class L, class P, class TP, int NT, class FV, class GV>
+__device__ __forceinline__ void edge_stores(const StepArgs<typename P::real>& a, const CellPos& e,
+                                            int col, FV fval, GV gval) {
+  using Real = typename P::real;
+  using TL = typename TracerLattice<L::D>::type;
+  auto* f = static_cast<typename P::type*>(a.f);
+#pragma unroll
+  for (int i = 0; i < L::Q; ++i) {
+    const int cz = comp<L>(i, 2);
+    if (cz == 0 || !is_edge(St::H, col, cz)) continue;
+    P::store_dev(f + (size_t)i * a.n + e.upstream<L>(i), fval(opp(i)), weight<L, Real>(i));
+  }
+  if constexpr (NT == 1) {
+    auto* g = static_cast<typename TP::type*>(a.tr[0].g);
+#pragma unroll
+    for (int i = 0; i < TL::Q; ++i) {
+      const int cz = comp<TL>(i, 2);
+      if (cz == 0 || !is_edge(St::HG, col, cz)) continue;
+      TP::store(g + (size_t)i * a.n + e.upstream<TL>(i), gval(opp(i)), 0.0f);
+    }
+  }
+}
+
+}  // namespace lbm
+
+// The two-cells-a-thread update, which writes through stage_pos.
+#include "aa_pair.cuh"
+
+namespace lbm {
+
 // update_cell's output into the stage it read from: slot i of the thread's cell on odd steps
-// (position i, column tid), slot i of the upstream cell on even steps of whole rows (the very
-// position the thread read, shifted and wrapped). A tile's slots then leave as whole row segments.
+// (position i, column tid), slot i of the upstream cell on even steps (the very position the
+// thread read: shifted, and wrapped when a row is one tile). The producer then writes the stage
+// back as row segments.
 template <class St, class L, class TL>
 struct StageSink {
+  using Real = typename St::Real;
   unsigned char* st;
   int tid;
+
   template <class LL, class P, bool EVEN, bool DEV>
   __device__ __forceinline__ void fluid(typename P::type*, long long, const CellPos&,
                                         const typename P::real (&v)[LL::Q]) const {
     using T = typename P::type;
-    using Real = typename P::real;
     T* base = reinterpret_cast<T*>(st);
 #pragma unroll
     for (int i = 0; i < LL::Q; ++i) {
-      T* p = base + i * St::SEG +
-             (EVEN ? St::H + ((tid - comp<LL>(i, 2)) & (kTmaTile - 1)) : tid);
+      T* p = base + i * St::SEG + stage_pos<St::kWR, EVEN>(St::H, tid, comp<LL>(i, 2));
       const Real val = EVEN ? v[opp(i)] : v[i];
       if constexpr (DEV)
         P::store_dev(p, val, weight<LL, Real>(i));
@@ -251,8 +317,7 @@ struct StageSink {
     TT* base = reinterpret_cast<TT*>(st + St::off_trc);
 #pragma unroll
     for (int i = 0; i < TLL::Q; ++i) {
-      TT* p = base + i * St::SEGG +
-              (EVEN ? St::HG + ((tid - comp<TLL>(i, 2)) & (kTmaTile - 1)) : tid);
+      TT* p = base + i * St::SEGG + stage_pos<St::kWR, EVEN>(St::HG, tid, comp<TLL>(i, 2));
       TP::store(p, EVEN ? v[opp(i)] : v[i], 0.0f);
     }
   }
@@ -275,10 +340,13 @@ __host__ __device__ constexpr int tma_threads() {
 // the compiler keeps more of each cell in registers (~90 for FP32 D3Q27, ~80 for the fused
 // D2Q9 + tracer even step) and two CTAs share an SM; measured 3-5% faster than three leaner CTAs.
 // 16-bit populations move half the bytes and need the occupancy instead: three CTAs for D3Q27,
-// four for D2Q9 (one CTA a SM cost them 15%).
+// four for D2Q9 (one CTA a SM cost them 15%). Two cells a thread: three CTAs for D3Q27, four for
+// D2Q9 (~95 registers; five or six CTAs cap them at 81 / 68 and measured 9% / 32% slower on the
+// FP16 channel).
 template <class L, int K, bool PAIR = false>
 constexpr int tma_min_blocks() {
-  return PAIR ? 3 : ((K == kF16 || K == kBF16) ? (L::Q >= 27 ? 3 : 4) : 1);
+  if constexpr (PAIR) return L::Q >= 27 ? 3 : 4;
+  return (K == kF16 || K == kBF16) ? (L::Q >= 27 ? 3 : 4) : 1;
 }
 
 // Warp-specialised: warps 0..7 consume (one cell per thread), warp 8 loads and stores stages.
@@ -336,17 +404,18 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
     }
   };
 
-  // WR: every row is one tile (nz == T; even steps only). Odd steps, and even steps of one-tile
-  // rows, leave their results in the stage, and the producer writes the stage back as whole row
-  // segments before refilling it (bulk stores). Other even steps store from registers (their
-  // results' segments are shifted by c_iz, so not 16-byte aligned) and release the stage warp by
-  // warp as soon as the operands are read. (Bulk stores of the aligned part with plain stores
-  // of the two partial chunks per slot were correct there but made the producer the limit on
-  // the 4096x2048 channel: no gain with FP32 populations, 8-17% slower with FP16.)
+  // WR: every row is one tile (nz == T; even steps only). Every step leaves its results in the
+  // stage, and the producer writes the stage back as row segments before refilling it (bulk
+  // stores): whole segments on odd steps and on even steps of one-tile rows; on other even
+  // steps, whose segments are shifted by c_iz, the 16-byte chunks wholly inside each segment,
+  // while the cells at the tile's ends store the few results outside them from their registers
+  // once their warp has released the stage (edge_range, edge_stores). (Per-thread stores of
+  // every result straight from registers cost ~100 integer instructions per cell for their
+  // addresses and made the 16-bit even step issue-bound; the producer storing the ragged ends
+  // made it the limit; the end cells storing them before the release held back every stage.)
   constexpr bool whole_row = WR;
-  constexpr bool bulk_out = !EVEN || WR;
   constexpr int CW = tma_consumer_warps<PAIR>();
-  static_assert(!PAIR || (bulk_out && NT == 0), "two cells a thread: results through the stage, no tracer");
+  static_assert(!PAIR || L::D == 2 || NT == 0, "two cells a thread in 3D: no tracer");
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(full + s, 1);
@@ -371,6 +440,23 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
       unsigned dst;               // byte offset inside a stage of element z0 - hl
       int kind;                   // 0 none, 1 row segment with halo, 2 own tile (no halo)
       bool gathered;              // moved by the four-row tensor copies instead (see below)
+      int so;                     // results: row elements [z0 + so, z0 + so + sbytes / es)
+      unsigned sdst, sbytes;      // from this stage byte offset
+    };
+    // The bulk-stored part of a row segment's results: the whole tile, or on even steps of rows
+    // longer than one tile the chunks of edge_range (the stage holds element z0 - h + k at
+    // index k, h = 16 / es).
+    auto set_store = [&](Job& jb, int cz) {
+      jb.so = 0;
+      jb.sdst = jb.dst;
+      jb.sbytes = (unsigned)(kTmaTile * jb.es);
+      if (EVEN && !whole_row) {
+        const int h = 16 / jb.es;
+        const EdgeRange r = edge_range(h, cz);
+        jb.so = (r.first - 1) * h;
+        jb.sdst = jb.dst + (unsigned)((r.first * h - (h - jb.hl)) * jb.es);
+        jb.sbytes = (unsigned)((r.last1 - r.first) * h * jb.es);
+      }
     };
     // Even steps of one-tile rows: the population slots travel four rows at a time
     // (tile::gather4 / scatter4 over the population array seen as rows of 256 cells, row
@@ -383,7 +469,7 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       const int op = lane + 32 * k;
-      Job jb{nullptr, 0, 0, 0, 0, 1, 0u, 0, false};
+      Job jb{nullptr, 0, 0, 0, 0, 1, 0u, 0, false, 0, 0u, 0u};
       if (op < Q) {
         const int slot = op;  // stage position op holds slot op (odd steps read opp(i) from it)
         const int cz = EVEN && !whole_row ? comp_rt<L, 2>(op) : 0;
@@ -397,6 +483,7 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
         jb.dst = (unsigned)(((size_t)op * St::SEG + St::H - jb.hl) * sizeof(T));
         jb.kind = 1;
         jb.gathered = by_rows;
+        set_store(jb, cz);
       } else if (op < Q + St::NG) {
         if constexpr (NT == 1) {
           const int i = op - Q;
@@ -410,6 +497,7 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
           jb.es = sizeof(TT);
           jb.dst = (unsigned)(St::off_trc + ((size_t)i * St::SEGG + St::HG - jb.hl) * sizeof(TT));
           jb.kind = 1;
+          set_store(jb, cz);
         }
       } else if (op == Q + St::NG) {
         if (a.acc_mode == kAccBoussinesq) {
@@ -457,10 +545,9 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
         r[m] = slot * a.nx * a.ny + ux * a.ny + uy;
       }
     };
-    // With bulk_out the consumers leave a tile's results in its stage: each population and
-    // tracer segment goes back to the row it came from (no halo then: odd steps read their own
-    // row, even steps of one-tile rows the whole row), and the stage is refilled once the
-    // stores have read it.
+    // The consumers leave a tile's results in its stage: each population and tracer segment
+    // goes back to the row it came from (set_store's part of it), and the stage is refilled once
+    // the stores have read it.
     TileWalker tws;
     tws.init(blockIdx.x, gridDim.x, a.ny, tiles_per_row);
     auto store_stage = [&](int s) {
@@ -483,10 +570,11 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
           const Job& jb = jobs[k];
-          if (jb.kind == 1 && !jb.gathered)
-            bulk_store(const_cast<unsigned char*>(job_row(jb, tws.x, tws.y)) +
-                           (size_t)tws.zt * kTmaTile * jb.es,
-                       st + jb.dst, (unsigned)(kTmaTile * jb.es));
+          if (jb.kind == 1 && !jb.gathered) {
+            unsigned char* row = const_cast<unsigned char*>(job_row(jb, tws.x, tws.y));
+            bulk_store(row + ((size_t)tws.zt * kTmaTile + jb.so) * jb.es, st + jb.sdst,
+                       jb.sbytes);
+          }
         }
       }
       bulk_commit();
@@ -502,7 +590,7 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
       const int s = j % S;
       if (j >= S) ok = mbar_wait(empty + s, (unsigned)(((j / S) - 1) & 1), a.spin_limit);
       if (!__all_sync(0xffffffffu, ok)) break;
-      if (j >= S && bulk_out) store_stage(s);
+      if (j >= S) store_stage(s);
       const int x = tw.x, y = tw.y, z0 = tw.zt * kTmaTile;
       unsigned char* st = stage_ptr(s);
       if (lane == 0) mbar_expect_tx(full + s, expect);
@@ -536,13 +624,13 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
       produced = j + 1;
     }
     // The last tiles' results (bounded waits for the consumers), then every store complete.
-    if (bulk_out && ok) {
+    if (ok) {
       for (int j = produced - S > 0 ? produced - S : 0; j < produced && ok; ++j) {
         ok = __all_sync(0xffffffffu, mbar_wait(empty + j % S, (unsigned)((j / S) & 1), a.spin_limit));
         if (ok) store_stage(j % S);
       }
     }
-    if (bulk_out) bulk_wait_all();
+    bulk_wait_all();
     if (!ok && lane == 0) atomicOr(a.status, 2);
     // Leave only once the copies of the last stages have landed (bounded), so that no copy
     // writes into shared memory after the CTA is gone.
@@ -553,8 +641,9 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
   }
 
   if constexpr (PAIR) {
-    // ---- consumer warps, two cells a thread: cells z0 + tid and z0 + tid + T/2 of every tile.
+    // ---- consumer warps, two cells a thread: cells z0 + col and z0 + col + T/2 of every tile.
     constexpr int HALF = kTmaTile / 2;
+    constexpr int QT = NT == 1 ? TL::Q : 1;
     TileWalker tw;
     tw.init(blockIdx.x, gridDim.x, a.ny, tiles_per_row);
     for (int j = 0; j < count; ++j, tw.next()) {
@@ -567,35 +656,60 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
       }
       const int x = tw.x, y = tw.y, z0 = tw.zt * kTmaTile;
       unsigned char* st = stage_ptr(s);
+      const int col = tid;  // this thread's columns: col and col + T/2
       float2 fv[Q];
 #pragma unroll
       for (int i = 0; i < Q; ++i) {
         const T* seg =
             reinterpret_cast<const T*>(st + (size_t)(EVEN ? i : opp(i)) * St::SEG * sizeof(T));
         const int cz = comp<L>(i, 2);
-        const int za = whole_row ? (tid - cz) & (kTmaTile - 1) : tid - cz;
-        const int zb = whole_row ? (tid + HALF - cz) & (kTmaTile - 1) : tid + HALF - cz;
-        const T va = EVEN ? seg[St::H + za] : seg[tid];
-        const T vb = EVEN ? seg[St::H + zb] : seg[tid + HALF];
+        const T va = seg[stage_pos<whole_row, EVEN>(St::H, col, cz)];
+        const T vb = seg[stage_pos<whole_row, EVEN>(St::H, col + HALF, cz)];
         fv[i] = make_float2(P::load_dev(&va, 0.0f), P::load_dev(&vb, 0.0f));
+      }
+      float2 gv[QT];
+      if constexpr (NT == 1) {
+#pragma unroll
+        for (int i = 0; i < St::NG; ++i) {
+          const TT* seg = reinterpret_cast<const TT*>(
+              st + St::off_trc + (size_t)(EVEN ? i : opp(i)) * St::SEGG * sizeof(TT));
+          const int cz = comp<TL>(i, 2);
+          gv[i] = make_float2(TP::load(seg + stage_pos<whole_row, EVEN>(St::HG, col, cz), 0.0f),
+                              TP::load(seg + stage_pos<whole_row, EVEN>(St::HG, col + HALF, cz),
+                                       0.0f));
+        }
       }
       const float2 cval =
           a.acc_mode == kAccBoussinesq
-              ? make_float2(reinterpret_cast<const Real*>(st + St::off_val)[tid],
-                            reinterpret_cast<const Real*>(st + St::off_val)[tid + HALF])
+              ? make_float2(reinterpret_cast<const Real*>(st + St::off_val)[col],
+                            reinterpret_cast<const Real*>(st + St::off_val)[col + HALF])
               : make_float2(0.0f, 0.0f);
-      const int flagA = st[St::off_flag + tid], flagB = st[St::off_flag + tid + HALF];
-      const unsigned row = (unsigned)x * (unsigned)a.ny * (unsigned)a.nz + (unsigned)y * (unsigned)a.nz;
-      update_cell2<St, L, TRT, K, EVEN, kTmaTile>(a, st, tid, row + z0 + tid, row + z0 + tid + HALF,
-                                                  flagA, flagB, fv, cval);
+      const int flagA = st[St::off_flag + col], flagB = st[St::off_flag + col + HALF];
+      const CellPos cA = make_cellpos(a, x, y, z0 + col, false);
+      const CellPos cB = make_cellpos(a, x, y, z0 + col + HALF, false);
+      // fv / gv hold the results afterwards (walls: untouched)
+      update_cell2<L, TRT, K, EVEN, NT, KT>(a, PairSink<St, kTmaTile>{st, col}, cA, cB, flagA,
+                                            flagB, fv, gv, cval);
       fence_proxy_async();  // this thread's stage writes, visible to the bulk stores
       __syncwarp();
       if (lane == 0) mbar_arrive(empty + s);
+      if constexpr (EVEN && !whole_row) {
+        // Cell A can only be at the tile's left end, cell B only at its right end.
+        constexpr int HE = St::H > St::HG ? St::H : St::HG;
+        const bool ea = col < HE && !(flagA & 1), eb = col + HALF >= kTmaTile - HE && !(flagB & 1);
+        if (ea || eb) {
+          const int ec = ea ? col : col + HALF;
+          const CellPos e = make_cellpos(a, x, y, z0 + ec, true);
+          edge_stores<St, L, P, TP, NT>(
+              a, e, ec, [&](int i) { return ea ? fv[i].x : fv[i].y; },
+              [&](int i) { return ea ? gv[i].x : gv[i].y; });
+        }
+      }
     }
     return;
   }
 
-  // ---- consumer warps: thread tid owns cell z0 + tid of every tile.
+  // ---- consumer warps: thread tid owns cell z0 + col of every tile.
   TileWalker tw;
   tw.init(blockIdx.x, gridDim.x, a.ny, tiles_per_row);
   for (int j = 0; j < count; ++j, tw.next()) {
@@ -607,14 +721,14 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
       break;  // the producer's own waits are bounded too
     }
     const int x = tw.x, y = tw.y, z0 = tw.zt * kTmaTile;
-    const unsigned char* st = stage_ptr(s);
+    unsigned char* st = stage_ptr(s);
+    const int col = tid;  // this thread's column
     Real fv[Q];
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
       const T* seg =
           reinterpret_cast<const T*>(st + (size_t)(EVEN ? i : opp(i)) * St::SEG * sizeof(T));
-      const int zi = whole_row ? (tid - comp<L>(i, 2)) & (kTmaTile - 1) : tid - comp<L>(i, 2);
-      const T v = EVEN ? seg[St::H + zi] : seg[tid];
+      const T v = seg[stage_pos<whole_row, EVEN>(St::H, col, comp<L>(i, 2))];
       if constexpr (dev_in<K>())
         fv[i] = P::load_dev(&v, weight<L, Real>(i));
       else
@@ -626,29 +740,30 @@ __global__ void __launch_bounds__(tma_threads<PAIR>(), tma_min_blocks<L, K, PAIR
       for (int i = 0; i < St::NG; ++i) {
         const TT* seg = reinterpret_cast<const TT*>(
             st + St::off_trc + (size_t)(EVEN ? i : opp(i)) * St::SEGG * sizeof(TT));
-        const int zi = whole_row ? (tid - comp<TL>(i, 2)) & (kTmaTile - 1) : tid - comp<TL>(i, 2);
-        g[i] = TP::load(EVEN ? seg + St::HG + zi : seg + tid, 0.0f);
+        g[i] = TP::load(seg + stage_pos<whole_row, EVEN>(St::HG, col, comp<TL>(i, 2)), 0.0f);
       }
     }
     const Real cval = a.acc_mode == kAccBoussinesq
-                          ? reinterpret_cast<const Real*>(st + St::off_val)[tid]
+                          ? reinterpret_cast<const Real*>(st + St::off_val)[col]
                           : Real(0);
-    const int flag = st[St::off_flag + tid];
-    const CellPos c = make_cellpos(a, x, y, z0 + tid, EVEN && !bulk_out);
-    if (!bulk_out) {
-      __syncwarp();
-      if (lane == 0) mbar_arrive(empty + s);  // this warp is done with stage s
-      update_cell<L, TRT, K, EVEN, NT, GlobalSink, KT>(a, c, flag, fv, g, cval, a.om_pos,
-                                                      a.om_neg);
-      continue;
-    }
-    // Results into the stage, where the producer picks them up as whole row segments.
-    const StageSink<St, L, TL> sink{const_cast<unsigned char*>(st), tid};
+    const int flag = st[St::off_flag + col];
+    const CellPos c = make_cellpos(a, x, y, z0 + col, false);
+    // Results into the stage, where the producer picks them up as row segments (fv / g hold
+    // them afterwards; walls: untouched).
+    const StageSink<St, L, TL> sink{st, col};
     update_cell<L, TRT, K, EVEN, NT, StageSink<St, L, TL>, KT>(a, c, flag, fv, g, cval, a.om_pos,
                                                               a.om_neg, sink);
     fence_proxy_async();  // this thread's stage writes, visible to the bulk stores
     __syncwarp();
     if (lane == 0) mbar_arrive(empty + s);
+    if constexpr (EVEN && !whole_row) {
+      constexpr int HE = St::H > St::HG ? St::H : St::HG;
+      if ((col < HE || col >= kTmaTile - HE) && !(flag & 1)) {
+        const CellPos e = make_cellpos(a, x, y, z0 + col, true);
+        edge_stores<St, L, P, TP, NT>(
+            a, e, col, [&](int i) { return fv[i]; }, [&](int i) { return g[i]; });
+      }
+    }
   }
 }
 

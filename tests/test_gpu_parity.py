@@ -331,6 +331,14 @@ TMA_CASES = {
                                           tracers=[["t0", ["bgk", 0.62]]],
                                           couplings=[["t0", 0.1, 0.5, [0.0, -0.01]]],
                                           calls=[2, 4]),
+    # Rows of several tiles: even steps write the stage back through the consumers' vector
+    # stores, including the ends of each segment that wrap to the row's other end.
+    "d2q9_bgk_gravity_long_rows": dict(counts=[12, 768], omega=["bgk", 0.55], walls=True,
+                                       gravity=[1e-3, -2e-3], calls=[2, 4]),
+    "d2q9_bgk_trt_tracer_long_rows": dict(counts=[10, 512], omega=["bgk", 0.6], walls=True,
+                                          tracers=[["t0", ["trt", 0.64]]],
+                                          couplings=[["t0", 0.1, 0.5, [0.0, -0.01]]],
+                                          calls=[2, 4]),
     "d3q27_bgk_walls_gravity": dict(counts=[5, 4, 256], omega=["bgk", 0.55], walls=True,
                                     gravity=[1e-3, 0.0, -1e-3], calls=[4]),
     "d3q27_trt_tracer_coupling": dict(counts=[3, 3, 256], omega=["trt", 0.58], walls=True,
@@ -401,13 +409,15 @@ def test_tma_path_f64_vs_oracle_f64(name):
 
 @pytest.mark.parametrize("storage", ["f32", "f16", "bf16", "f64"])
 @pytest.mark.parametrize("name", ["d2q9_trt_tracer_coupling", "d2q9_trt_tracer_one_tile_rows",
+                                  "d2q9_bgk_gravity_long_rows", "d2q9_bgk_trt_tracer_long_rows",
                                   "d3q27_trt_tracer_coupling", "d3q27_single_row",
                                   "d3q27_bgk_walls_gravity"])
 def test_staged_path_bit_identical_to_direct(name, storage):
     """The TMA-staged kernel (row copies, tensor-map boxes, four-row gathers on one-tile rows,
-    results stored through the stage; two cells a thread for D3Q27 BGK with 16-bit storage and
-    no tracer) and the direct kernel run the same cell update: every storage type gives the
-    same bits on both paths, for even and odd steps."""
+    results written back through the stage by bulk stores or by the consumers; two cells a
+    thread with 16-bit storage for D3Q27 BGK without a tracer and for D2Q9 with or without one)
+    and the direct kernel run the same cell update: every storage type gives the same bits on
+    both paths, for even and odd steps."""
     from tests.golden.make_golden import seeded_inputs
 
     spec = TMA_CASES[name]
