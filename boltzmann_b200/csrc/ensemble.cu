@@ -195,18 +195,28 @@ __global__ void __launch_bounds__(kRowThreads)
 
   if (warp == CW) {
     // ---- producer warp: lane k < 9 copies slot k, lane 9 the flags.
+    // Row descriptors are loaded two rows ahead and domain descriptors one row ahead, so that
+    // the dependent table loads never hold up the copies of the next row.
+    const long long r0 = blockIdx.x, dr = gridDim.x;
+    RowDesc rd_next{0, 0}, rd_after{0, 0};
+    DomainDesc dom_next{0, 1, 1, 0.0f, 0.0f};
+    if (count > 0) rd_next = e.rows[r0];
+    if (count > 1) rd_after = e.rows[r0 + dr];
+    if (count > 0) dom_next = e.domains[rd_next.domain];
     bool ok = true;
     int produced = 0;
     for (int j = 0; j < count && ok; ++j) {
       const int s = j % S;
+      const RowDesc rd = rd_next;
+      const DomainDesc dom = dom_next;
+      rd_next = rd_after;
+      if (j + 2 < count) rd_after = e.rows[r0 + (long long)(j + 2) * dr];
+      if (j + 1 < count) dom_next = e.domains[rd_next.domain];
       if (j >= S) ok = mbar_wait(empty + s, (unsigned)(((j / S) - 1) & 1), a.spin_limit);
       if (!__all_sync(0xffffffffu, ok)) {
         ok = false;
         break;
       }
-      const long long r = blockIdx.x + (long long)j * gridDim.x;
-      const RowDesc rd = e.rows[r];
-      const DomainDesc dom = e.domains[rd.domain];
       const unsigned ny = (unsigned)dom.ny;
       const unsigned rowx = (unsigned)dom.base + (unsigned)rd.x * ny;
       const unsigned rowm = (unsigned)dom.base + (unsigned)(rd.x == 0 ? dom.nx - 1 : rd.x - 1) * ny;
