@@ -333,6 +333,10 @@ def run_ours(args) -> None:
     # Device-timed run: inputs resident in HBM, only the AA kernels in the timed region.
     sim = build_sim(setup, args.storage, args.tracer_storage)
     sim.iterate(2 * W)  # upload, equilibrate, warm-up steps
+    # One untimed call of the timed length: the library captures the CUDA graphs a call of that
+    # many steps replays once per simulation state, and that one-time capture stays out of the
+    # timed region.
+    sim._iterate_device(2 * K)
     stream = torch.cuda.ExternalStream(sim._stream())
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()

@@ -102,7 +102,16 @@ int check_status(lbm_sim* s) {
   return LBM_OK;
 }
 
+// The captured step graphs no longer match the simulation's state.
+void drop_graph(lbm_sim* s) {
+  for (const lbm_sim::StepGraph& g : s->graphs) cudaGraphExecDestroy(g.exec);
+  s->graphs.clear();
+  s->graph_warm = false;
+  s->graph_failed = false;
+}
+
 void release(lbm_sim* s) {
+  drop_graph(s);
   for (lbm_sim::Tracer& t : s->tracers) {
     cudaFree(t.g);
     cudaFree(t.val);
@@ -113,6 +122,64 @@ void release(lbm_sim* s) {
   cudaFree(s->flags);
   cudaFree(s->status);
   if (s->stream) cudaStreamDestroy(s->stream);
+}
+
+}  // namespace
+
+namespace {
+
+// Step pairs in one captured graph: at most kGraphPairs, at least kMinGraphPairs. Small domains
+// take a few microseconds a step, as long as a launch takes on the host, and a replayed graph
+// issues its launches back to back; but a replay has a start-up latency of its own on the GPU,
+// which shorter graphs do not repay (a learned closure's loop of 10-step calls between its own
+// kernels measured 5% slower with graphs of 4 pairs).
+constexpr int64_t kGraphPairs = 16, kMinGraphPairs = 8;
+
+// One AA step pair (even, odd); the odd step writes rho / vel when `last`
+// (src/simulation.rs:350: even steps are the iteration counter's even values).
+cudaError_t launch_pair(lbm_sim* s, bool last) {
+  for (int k = 0; k < 2; ++k) {
+    const bool even = k == 0, moments = last && !even;
+    const cudaError_t e = s->dim == 2 ? lbm::launch_step_d2q9(*s, even, moments)
+                                      : lbm::launch_step_d3q27(*s, even, moments);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// The graph of `pairs` step pairs (no moments written), captured from the simulation's stream if
+// it is not cached yet; null when the capture fails. The launch counters the capture advanced are
+// put back and kept per replay.
+const lbm_sim::StepGraph* step_graph(lbm_sim* s, int64_t pairs) {
+  for (const lbm_sim::StepGraph& g : s->graphs)
+    if (g.pairs == pairs) return &g;
+  if (s->graphs.size() >= 4) {
+    cudaGraphExecDestroy(s->graphs.front().exec);
+    s->graphs.erase(s->graphs.begin());
+  }
+  lbm_sim::StepGraph g{pairs, nullptr, {0, 0}};
+  const int64_t before[2] = {s->launches[0], s->launches[1]};
+  cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return nullptr;
+  cudaError_t le = cudaSuccess;
+  for (int64_t p = 0; p < pairs && le == cudaSuccess; ++p) le = launch_pair(s, false);
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamEndCapture(s->stream, &graph);
+  for (int k = 0; k < 2; ++k) {
+    g.launches[k] = s->launches[k] - before[k];
+    s->launches[k] = before[k];
+  }
+  if (le == cudaSuccess && e == cudaSuccess) e = cudaGraphInstantiate(&g.exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (le != cudaSuccess || e != cudaSuccess) return nullptr;
+  s->graphs.push_back(g);
+  return &s->graphs.back();
+}
+
+int step_launch_fail(cudaError_t e) {
+  if (e == cudaErrorNotSupported)
+    return fail(LBM_ERR_UNSUPPORTED, "16-bit tracer storage takes one tracer");
+  return cuda_fail(e, "AA step launch");
 }
 
 }  // namespace
@@ -247,6 +314,7 @@ int lbm_add_tracer(lbm_sim* sim, int q, int collision, float omega_pos, float om
   LBM_CUDA(cudaMemsetAsync(t.g, 0, (size_t)sim->n * q * gb, sim->stream));
   LBM_CUDA(cudaMemsetAsync(t.val, 0, (size_t)sim->n * rb, sim->stream));
   sim->tracers.push_back(t);
+  drop_graph(sim);
   if (out_index) *out_index = (int)sim->tracers.size() - 1;
   return LBM_OK;
 }
@@ -257,10 +325,12 @@ int lbm_set_tracer_storage(lbm_sim* sim, int storage) {
     return fail(LBM_ERR_STATE, "the tracer storage is chosen before the first tracer is added");
   if (storage == LBM_STORAGE_F32 && sim->storage != LBM_STORAGE_F64) {
     sim->tracer_storage = -1;
+    drop_graph(sim);
     return LBM_OK;
   }
   if ((storage == LBM_STORAGE_F16 || storage == LBM_STORAGE_BF16) && storage == sim->storage) {
     sim->tracer_storage = storage;
+    drop_graph(sim);
     return LBM_OK;
   }
   return fail(LBM_ERR_UNSUPPORTED,
@@ -271,6 +341,7 @@ int lbm_set_gravity(lbm_sim* sim, const float* g) {
   if (int rc = activate(sim)) return rc;
   if (g == nullptr) return fail(LBM_ERR_ARGUMENT, "null gravity");
   sim->has_gravity = true;
+  drop_graph(sim);
   for (int k = 0; k < sim->dim; ++k) sim->gravity[k] = g[k];
   return LBM_OK;
 }
@@ -285,6 +356,7 @@ int lbm_add_coupling(lbm_sim* sim, int tracer, float alpha, float c0, const floa
   c.c0 = c0;
   for (int k = 0; k < sim->dim; ++k) c.g[k] = g[k];
   sim->couplings.push_back(c);
+  drop_graph(sim);
   return LBM_OK;
 }
 
@@ -386,15 +458,37 @@ int lbm_iterate(lbm_sim* sim, int64_t iters) {
     if (!tracer_kernel(sim->dim, t.q, t.collision))
       return fail(LBM_ERR_UNSUPPORTED, "Kernel not found: D" + std::to_string(sim->dim) + "Q" +
                                            std::to_string(t.q) + " AdvectionDiffusion");
-  for (int64_t it = 0; it < iters; ++it) {
-    const bool even = (it % 2) == 0;  // src/simulation.rs:350
-    const bool last = it == iters - 1;
-    cudaError_t e = sim->dim == 2 ? lbm::launch_step_d2q9(*sim, even, last)
-                                  : lbm::launch_step_d3q27(*sim, even, last);
-    if (e == cudaErrorNotSupported)
-      return fail(LBM_ERR_UNSUPPORTED, "16-bit tracer storage takes one tracer");
-    if (e != cudaSuccess) return cuda_fail(e, "AA step launch");
+  int64_t left = iters / 2;  // step pairs
+  // The pairs before the last one (which writes the moments) go out as replays of captured
+  // graphs of kMinGraphPairs..kGraphPairs pairs while that many are left; the rest are launched
+  // directly, and so is the first pair after creation or a change of state (outside any capture,
+  // so each kernel's one-time set-up has run). Not while the caller is capturing the simulation's
+  // stream into a graph of its own.
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  const bool outer = cudaStreamIsCapturing(sim->stream, &cs) == cudaSuccess &&
+                     cs != cudaStreamCaptureStatusNone;
+  if (!outer && !sim->graph_failed && left >= kMinGraphPairs + 2) {
+    if (!sim->graph_warm) {
+      if (cudaError_t e = launch_pair(sim, false)) return step_launch_fail(e);
+      --left;
+      sim->graph_warm = true;
+    }
+    while (left - 1 >= kMinGraphPairs) {
+      const int64_t pairs = left - 1 < kGraphPairs ? left - 1 : kGraphPairs;
+      const lbm_sim::StepGraph* g = step_graph(sim, pairs);
+      if (g == nullptr) {  // launched one at a time from now on, until the state changes
+        cudaGetLastError();
+        sim->graph_failed = true;
+        break;
+      }
+      LBM_CUDA(cudaGraphLaunch(g->exec, sim->stream));
+      sim->launches[0] += g->launches[0];
+      sim->launches[1] += g->launches[1];
+      left -= pairs;
+    }
   }
+  for (; left > 0; --left)
+    if (cudaError_t e = launch_pair(sim, left == 1)) return step_launch_fail(e);
   return LBM_OK;
 }
 
@@ -461,12 +555,14 @@ int lbm_set_kernel_path(lbm_sim* sim, int path) {
   if (int rc = activate(sim)) return rc;
   if (path < LBM_PATH_AUTO || path > LBM_PATH_STAGED)
     return fail(LBM_ERR_ARGUMENT, "unknown kernel path");
+  if (sim->kernel_path != path) drop_graph(sim);
   sim->kernel_path = path;
   return LBM_OK;
 }
 
 int lbm_set_spin_limit(lbm_sim* sim, int64_t polls) {
   if (int rc = activate(sim)) return rc;
+  if (sim->spin_limit != (polls < 0 ? -1 : polls)) drop_graph(sim);
   sim->spin_limit = polls < 0 ? -1 : polls;
   return LBM_OK;
 }
@@ -482,6 +578,7 @@ int lbm_set_omega_field(lbm_sim* sim, const float* field) {
   if (int rc = activate(sim)) return rc;
   if (field != nullptr && sim->storage == LBM_STORAGE_F64)
     return fail(LBM_ERR_UNSUPPORTED, "per-cell relaxation needs a float storage kind");
+  if (sim->omega_field != field) drop_graph(sim);
   sim->omega_field = field;
   return LBM_OK;
 }

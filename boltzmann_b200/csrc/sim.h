@@ -35,6 +35,16 @@ struct lbm_sim {
   int64_t spin_limit = -1;  // polls of the staged kernel's pipeline waits; < 0: the default
   // AA step launches since creation, per kernel variant: [0] direct, [1] TMA-staged.
   mutable int64_t launches[2] = {0, 0};
+  // Step pairs captured as CUDA graphs and replayed by lbm_iterate, one per pair count (at most
+  // four), dropped whenever a setter changes what a step launches; `warm` once a pair has run
+  // outside any capture in the current state (each kernel's one-time launch set-up done).
+  struct StepGraph {
+    int64_t pairs;
+    cudaGraphExec_t exec;
+    int64_t launches[2];  // what one replay adds to `launches`
+  };
+  std::vector<StepGraph> graphs;
+  bool graph_warm = false, graph_failed = false;
   const float* omega_field = nullptr;  // caller-owned per-cell om_pos, or null
 
   void* f = nullptr;    // [q][N] populations in the storage type

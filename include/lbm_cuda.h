@@ -134,7 +134,11 @@ LBM_API int lbm_download_g(lbm_sim* sim, int tracer, float* g);
 
 /* Advances `iters` AA steps (the per-step loop of Simulation::iterate,
  * src/simulation.rs:288-433). iters must be even (src/simulation.rs:279-281). Asynchronous:
- * returns once the steps are enqueued on the simulation's stream. */
+ * returns once the steps are enqueued on the simulation's stream. The step pairs before the
+ * last go out as replays of CUDA graphs of 8 to 16 pairs while that many are left, each graph
+ * captured once per simulation state; the rest, and the first pair after creation or after a
+ * setter changed the state, are launched directly, as is every step of a call made while the
+ * caller captures the simulation's stream. */
 LBM_API int lbm_iterate(lbm_sim* sim, int64_t iters);
 
 /* Device -> host copies after an iterate call (Fluid/Scalar::read_to_host,
