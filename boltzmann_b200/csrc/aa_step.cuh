@@ -489,6 +489,20 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
     const Real rinv = __frcp_rn(r);  // one correctly rounded reciprocal; u within 1.5 ulp
 #pragma unroll
     for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] = mul_r(u[ax], rinv);
+  } else if constexpr (sizeof(Real) == 4) {
+    // u = m / r, correctly rounded, from one correctly rounded reciprocal y = 1/r shared by the
+    // components: q = m y, then Markstein's quotient correction q + (m - r q) y, both steps
+    // fused multiply-adds (P. Markstein, "Computation of elementary functions on the IBM
+    // RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990). With y correctly rounded the
+    // corrected q is the correctly rounded quotient, so the bits are those of a division
+    // (tests/test_quotient_cpu.py checks the method against exact arithmetic); two divisions
+    // cost the issue-bound FP32 ensemble kernel 4.7%. (m y alone is biased for r near 1.)
+    const float y = __frcp_rn(r);
+#pragma unroll
+    for (int ax = 3 - L::D; ax < 3; ++ax) {
+      const float q = __fmul_rn(u[ax], y);
+      u[ax] = __fmaf_rn(__fmaf_rn(-r, q, u[ax]), y, q);
+    }
   } else {
 #pragma unroll
     for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] = u[ax] / r;
