@@ -437,8 +437,10 @@ __device__ __forceinline__ CellPos make_cellpos(const StepArgs<Real>& a, int x, 
 // om_pos / om_neg are the relaxation rates of the cell's domain (a.om_pos / a.om_neg for a single
 // simulation; per domain in an ensemble).
 // KT: storage kind of the fused tracers' populations (TracerPop).
+// UNFORCED: no body force, coupling or relaxation field by construction (batched ensembles), so
+// their per-cell checks are left out (+5% on the FP16 ensemble kernel).
 template <class L, bool TRT, int K, bool EVEN, int NT, class Sink = GlobalSink,
-          int KT = default_tracer_kind<K>()>
+          int KT = default_tracer_kind<K>(), bool UNFORCED = false>
 __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real>& a,
                                             const CellPos& c, int flag,
                                             typename Pop<K>::real (&f)[L::Q],
@@ -509,9 +511,10 @@ __device__ __forceinline__ void update_cell(const StepArgs<typename Pop<K>::real
   }
 
   // A per-cell relaxation field replaces the domain's om_pos (the force shift keeps the domain's).
-  if (a.omega_field != nullptr) om_pos = (Real)__ldg(a.omega_field + c.cell);
+  if (!UNFORCED && a.omega_field != nullptr) om_pos = (Real)__ldg(a.omega_field + c.cell);
   // Force as a velocity shift acc / omega (src/lib.cl:253-256; TRT: omega+, 682-685).
-  if (a.acc_mode == kAccConstant) {
+  if (UNFORCED) {
+  } else if (a.acc_mode == kAccConstant) {
 #pragma unroll
     for (int ax = 3 - L::D; ax < 3; ++ax) u[ax] = add_r(u[ax], a.force[ax]);
   } else if (a.acc_mode == kAccBoussinesq) {

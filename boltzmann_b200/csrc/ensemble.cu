@@ -357,11 +357,13 @@ __global__ void __launch_bounds__(kRowThreads)
           fv[i] = P::load(seg[slot] + zi, weight<D2Q9, Real>(i));
       }
       Real g[1];
+      // (ensembles carry no body force, coupling or relaxation field)
       if constexpr (sizeof(T) == 4)
-        update_cell<D2Q9, TRT, K, EVEN, 0, RowStoreSink<K>>(a, c, flag, fv, g, Real(0), om_p,
-                                                            om_n, RowStoreSink<K>{out_rows});
+        update_cell<D2Q9, TRT, K, EVEN, 0, RowStoreSink<K>, default_tracer_kind<K>(), true>(
+            a, c, flag, fv, g, Real(0), om_p, om_n, RowStoreSink<K>{out_rows});
       else
-        update_cell<D2Q9, TRT, K, EVEN, 0>(a, c, flag, fv, g, Real(0), om_p, om_n);
+        update_cell<D2Q9, TRT, K, EVEN, 0, GlobalSink, default_tracer_kind<K>(), true>(
+            a, c, flag, fv, g, Real(0), om_p, om_n);
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(empty + s);  // this warp is done with stage s
